@@ -1,0 +1,268 @@
+"""Benchmark: the intersection microbench (plain per-frame launch of pt_trace).
+
+Workload: a displaced icosphere subdivided 8 times (1,310,720 faces, radius 1, 3-octave value
+noise amplitude 0.05, seed 7) and 16,777,216 rays (origins uniform on a radius-3 sphere,
+directions toward uniform points of the unit ball, seed 11; even rays closest-hit, odd rays any-hit
+with tmax = distance to the target).  One step traces every ray once.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  `value` is Mrays/s with rays already in HBM (device pointers);
+`e2e` is the same through the C ABI with pinned host buffers (copies inside the timed region).
+`roofline.achieved` counts the reference algorithm's bytes per ray (32 B per node test, 44 B per
+face test, 28 B ray in, 16 B hit out) from the per-ray test counts of one counted pass.
+With N > 1 every rank traces its own full ray set against a replica of the scene (weak scaling,
+no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_RAYS = 16_777_216
+WORKLOAD = "intersection microbench: icosphere-8 displaced (1,310,720 tris), 16,777,216 rays (half any-hit)"
+
+
+def clocks_sampler():
+    """Sample SM clocks and throttle reasons with nvidia-smi while the timed region runs."""
+    q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+    idx = os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or "0"
+    try:
+        p = subprocess.Popen(["nvidia-smi", f"--id={idx}", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    except (FileNotFoundError, OSError):
+        return None
+    lines = []
+    t = threading.Thread(target=lambda: lines.extend(iter(p.stdout.readline, "")), daemon=True)
+    t.start()
+    return p, lines, t
+
+
+def clocks_summary(handle):
+    if handle is None:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+    p, lines, t = handle
+    p.terminate()
+    try:
+        p.wait(timeout=5)
+    except subprocess.TimeoutExpired:
+        p.kill()
+    t.join(timeout=2)
+    sm, mx, reasons = [], [], set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for ln in lines:
+        parts = [x.strip() for x in ln.split(",")]
+        if len(parts) < 7:
+            continue
+        try:
+            sm.append(float(parts[0]))
+            mx.append(float(parts[1]))
+        except ValueError:
+            continue
+        for nm, v in zip(names, parts[3:7]):
+            if v.lower() == "active":
+                reasons.add(nm)
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+            "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """DRAM bytes per launch of the trace kernel from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "trace_kernel_microbench.json")) as f:
+            return json.load(f).get("dram_bytes_per_launch_full_size")
+    except (OSError, ValueError):
+        return None
+
+
+def make_workload(n_rays):
+    from polytope_b200 import workloads as W
+    return W.microbench(n_rays=n_rays)
+
+
+def cpu_reference(meshes, rays, sample, threads):
+    """Time the reference's own closest/any-hit queries (oracle/_ref, else the restatement)."""
+    from oracle import pyoracle as po
+    if po.ref_available():
+        scene, kind = po.RefScene(meshes), "reference"
+    else:
+        scene, kind = po.OracleScene(meshes), "port"
+    sub = rays[:sample]
+    t0 = time.perf_counter()
+    scene.trace(sub, threads=threads)
+    dt = time.perf_counter() - t0
+    return sample / dt / 1e6, kind, dt
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    meshes, rays = make_workload(N_RAYS)
+    sample = args.ref_sample
+    for _ in range(max(0, args.warmup)):
+        cpu_reference(meshes, rays, min(sample, 65536), threads)
+    vals = []
+    for _ in range(args.steps):
+        v, kind, dt = cpu_reference(meshes, rays, sample, threads)
+        vals.append(v)
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": "Mrays/s", "value": round(value, 4), "unit": "Mrays/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rays_per_step": sample, "threads": threads},
+        "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": threads, "kind": kind,
+                         "sample": f"first {sample} rays of the {N_RAYS}-ray set per step, all host threads"},
+        "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--rays", type=int, default=N_RAYS)
+    ap.add_argument("--ref-sample", type=int, default=N_RAYS)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    import polytope_b200 as pb
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    meshes, rays = make_workload(args.rays)
+    n = len(rays)
+    scene = pb.Scene(meshes)
+    stream = torch.cuda.Stream(device=dev)
+
+    # counted pass (untimed): per-ray node / face tests for the algorithmic-bytes numerator
+    hits_np, nt, tt = scene.intersect(rays, counts=True)
+    alg_bytes = float(32 * nt.sum(dtype=np.uint64) + 44 * tt.sum(dtype=np.uint64) + (28 + 16) * n)
+
+    d_rays = torch.from_numpy(rays.view(np.uint8)).to(dev)
+    d_hits = torch.zeros(n * 16, dtype=torch.uint8, device=dev)
+
+    def step():
+        pb.check(pb.lib.pt_trace(scene.handle, d_rays.data_ptr(), n, d_hits.data_ptr(), pb.MEM_DEVICE, stream.cuda_stream))
+
+    with torch.cuda.stream(stream):
+        for _ in range(max(3, args.warmup)):
+            step()
+    stream.synchronize()
+    assert d_hits.cpu().numpy().tobytes() == hits_np.tobytes(), "device-resident hits differ from the counted pass"
+
+    sampler = clocks_sampler()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with torch.cuda.stream(stream):
+        ev[0].record(stream)
+        for k in range(args.steps):
+            step()
+            ev[k + 1].record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    per = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[-1])
+
+    # end to end through the C ABI with pinned host buffers (H2D + kernel + D2H per step)
+    h_rays = torch.from_numpy(rays.view(np.uint8)).pin_memory()
+    h_hits = torch.zeros(n * 16, dtype=torch.uint8).pin_memory()
+    for _ in range(2):
+        pb.check(pb.lib.pt_trace(scene.handle, h_rays.data_ptr(), n, h_hits.data_ptr(), 0, None))
+    e2e_steps = max(3, min(args.steps, 10))
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(e2e_steps):
+        pb.check(pb.lib.pt_trace(scene.handle, h_rays.data_ptr(), n, h_hits.data_ptr(), 0, None))
+    e1.record()
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    assert h_hits.numpy().tobytes() == hits_np.tobytes(), "e2e hits differ"
+    clk = clocks_summary(sampler)
+
+    ms = total_ms / args.steps
+    if dist:
+        t = torch.tensor([ms, e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, e2e_ms = float(t[0]), float(t[1])
+    if rank == 0:
+        value = n * world / (ms * 1e-3) / 1e6
+        e2e = n * world / (e2e_ms * 1e-3) / 1e6
+        peak, peak_kind = peaks()
+        achieved = alg_bytes / (ms * 1e-3) / 1e9
+        traffic = profiled_traffic()
+        line = {
+            "metric": "Mrays/s", "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": round(ms, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded generators)",
+            "config": {"workload": WORKLOAD, "rays_per_gpu": n, "faces": int(sum(len(m.faces) for m in meshes)),
+                       "launch": "plain per-frame launch (one trace kernel over all rays)",
+                       "l2": "inputs larger than L2 (rays 512 MiB + hits 256 MiB per step); BVH + faces (113 MB) stay L2-resident",
+                       "parallelism": f"replicas x{world}"},
+            "gpu_launches": args.steps,
+            "e2e": {"value": round(e2e, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 32 * n, "d2h_bytes_per_step": 16 * n,
+                    "ms_per_step": round(e2e_ms, 4)},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "note": f"algorithmic bytes {alg_bytes / 1e9:.2f} GB per launch (reference node/face test counts); peak {peak_kind}"},
+            "clocks": clk,
+            "step_ms": {"min": round(min(per), 4), "median": round(statistics.median(per), 4), "max": round(max(per), 4)},
+        }
+        if not args.no_cpu_baseline:
+            threads = os.cpu_count() or 1
+            v, kind, dt = cpu_reference(meshes, rays, args.ref_sample, threads)
+            line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mrays/s", "cores": threads, "kind": kind,
+                                    "sample": f"first {args.ref_sample} rays of the ray set ({dt:.1f} s)"}
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

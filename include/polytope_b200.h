@@ -1,0 +1,235 @@
+/*
+ * polytope_b200.h — C ABI of the B200 (sm_100a) ray/path-tracing hot path.
+ *
+ * This header is the drop-in boundary for Polytope's CPU render call.  The reference has no
+ * plugin/FFI layer; its boundary is a set of C++ classes.  Each entry point below names the
+ * reference interface it replaces (paths are relative to the Polytope source tree):
+ *
+ *   pt_bvh_build      <- poly::bvh::bound + poly::bvh::compact      src/cpu/acceleration/bvh.cpp:36-395, 652-698
+ *   pt_scene_create   <- poly::Scene (Shapes, Lights, Skybox, bvh_root) after compact()
+ *                                                                   src/cpu/scenes/Scene.h:17-35
+ *   pt_trace          <- poly::Scene::intersect -> bvh::intersect_compact -> Mesh::intersect
+ *                                                                   src/cpu/scenes/Scene.cpp:12-31,
+ *                                                                   src/cpu/acceleration/bvh.cpp:476-523,
+ *                                                                   src/cpu/shapes/mesh.cpp:161-355
+ *   pt_render         <- spawn N x AbstractRunner::Run + join + Output()
+ *                        (TileRunner::Run -> AbstractRunner::Trace -> PathTraceIntegrator::GetSample)
+ *                                                                   src/cpu/main.cpp:187-220,
+ *                                                                   src/cpu/runners/TileRunner.cpp:64-104,
+ *                                                                   src/cpu/runners/AbstractRunner.cpp:11-31,
+ *                                                                   src/cpu/integrators/PathTraceIntegrator.cpp:10-135
+ *
+ * Conventions
+ *   - Every function returns PT_OK (0) or a negative PT_E* status and never exits the process
+ *     (the reference calls exit(1) from ERROR, src/common/utilities/Common.h:13).  The message of
+ *     the last failure on the calling thread is returned by pt_last_error().
+ *   - Scene handles are immutable after pt_scene_create; concurrent pt_trace / pt_render calls on
+ *     one handle from several host threads (on different streams) are safe.
+ *   - `stream` arguments are cudaStream_t values passed as void* (NULL = legacy default stream).
+ *   - There is no CPU fallback: without a usable CUDA device every call that launches work
+ *     returns PT_ECUDA.
+ */
+#ifndef POLYTOPE_B200_H
+#define POLYTOPE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------------------------ */
+#define PT_OK        0
+#define PT_EINVAL   (-1)   /* bad argument, malformed tree, size out of range              */
+#define PT_ENOMEM   (-2)   /* host or device allocation failed                             */
+#define PT_ETIMEOUT (-3)   /* a bounded device wait ran out                                */
+#define PT_ECUDA    (-4)   /* CUDA runtime error or no device                              */
+#define PT_ESTACK   (-5)   /* traversal stack capacity exceeded (tree deeper than capacity) */
+
+/* ---- geometry ---------------------------------------------------------------------------- */
+
+/* One compacted BVH node, byte-identical to poly::compact_bvh_node (src/cpu/acceleration/bvh.h:24-53):
+ * bounding box p0,p1 (24 B), a union of high_child_offset (interior: the high child sits at
+ * this index + offset; the low child at this index + 1) and face_index_offset (leaf: first entry
+ * of the leaf-ordered face list), num_faces (0 for interior nodes) and the split axis. */
+typedef struct pt_bvh_node {
+    float    bb_min[3];
+    float    bb_max[3];
+    uint32_t offset;
+    uint16_t num_faces;
+    uint16_t axis;
+} pt_bvh_node;
+
+/* Materials (src/cpu/shading/brdf/abstract_brdf.h:15-20 BRDF_TYPE; Lambert = 1, Mirror = 2). */
+#define PT_MAT_LAMBERT 1u
+#define PT_MAT_MIRROR  2u
+
+/* One mesh instance: poly::Mesh + poly::mesh_geometry (src/cpu/shapes/mesh.h:17-113).
+ * Vertices are the *packed* arrays (x_packed...) indexed by fv0/fv1/fv2.  object_to_world is the
+ * row-major 4x4 poly::Transform::Matrix; world_to_object its Inverse (used only for vertex
+ * normals, src/cpu/structures/Transform.cpp:135-143).  A mesh with is_light != 0 is an area
+ * emitter (poly::Mesh::spd, mesh.h:99-109); emission is in the reference's x255 domain. */
+typedef struct pt_mesh_desc {
+    const float    *x, *y, *z;          /* packed vertex positions, num_vertices each          */
+    uint32_t        num_vertices;
+    const uint32_t *fv0, *fv1, *fv2;    /* per-face vertex indices, num_faces each             */
+    uint32_t        num_faces;
+    const float    *nx, *ny, *nz;       /* optional packed vertex normals (NULL if none)        */
+    float           object_to_world[16];
+    float           world_to_object[16];
+    uint32_t        material;           /* PT_MAT_LAMBERT or PT_MAT_MIRROR                      */
+    float           albedo[3];          /* Lambert reflectance or mirror Kr                     */
+    int32_t         is_light;
+    float           emission[3];
+} pt_mesh_desc;
+
+/* A scene: meshes in poly::Scene::Shapes order plus an optional constant environment
+ * (poly::ColorSkybox, src/cpu/scenes/skyboxes/ColorSkybox.cpp:8-10).  If `nodes` is non-NULL the
+ * caller passes the tree its own poly::bvh::compact() produced (nodes + leaf_ordered_indices as
+ * (mesh, face) uint32 pairs); otherwise pt_scene_create builds it with pt_bvh_build. */
+typedef struct pt_scene_desc {
+    const pt_mesh_desc *meshes;
+    uint32_t            num_meshes;
+    const pt_bvh_node  *nodes;          /* optional */
+    uint32_t            num_nodes;
+    const uint32_t     *leaf_pairs;     /* optional, 2 * (total faces) entries                  */
+    int32_t             has_env;
+    float               env[3];
+} pt_scene_desc;
+
+typedef struct pt_scene pt_scene;
+
+/* Global primitive ids: the faces of mesh m are numbered prim_base[m] + face, with prim_base the
+ * exclusive prefix sum of num_faces in mesh order (the order of poly::bvh::master_indices,
+ * bvh.cpp:45-118). */
+#define PT_PRIM_NONE 0xFFFFFFFFu
+
+/* Build the reference's SAH BVH (12-bucket binned SAH, BFS, bvh.cpp:36-395) and DFS-compact it
+ * (bvh.cpp:652-698) on the host.  The result is node-for-node and byte-for-byte identical to the
+ * reference.  nodes_out must hold *num_nodes_out entries on input (query the count first with
+ * nodes_out == NULL); leaf_pairs_out must hold 2 * total faces entries.  threads <= 0 = all cores. */
+int pt_bvh_build(const pt_mesh_desc *meshes, uint32_t num_meshes, int threads,
+                 pt_bvh_node *nodes_out, uint32_t *num_nodes_out, uint32_t *leaf_pairs_out);
+
+/* Upload a scene to the current CUDA device.  The descriptor's arrays are copied; the caller may
+ * free them on return. */
+int pt_scene_create(const pt_scene_desc *desc, pt_scene **out);
+int pt_scene_destroy(pt_scene *scene);
+
+typedef struct pt_scene_info {
+    uint32_t num_nodes;
+    uint32_t num_prims;
+    uint32_t num_meshes;
+    uint32_t max_depth;            /* deepest node level (root = 0)                           */
+    uint64_t device_bytes;         /* device memory held by the handle                        */
+} pt_scene_info;
+int pt_scene_get_info(const pt_scene *scene, pt_scene_info *info);
+
+/* ---- ray queries (Scene::intersect) ------------------------------------------------------ */
+
+/* A ray: origin, tmax (poly::Ray::MinT at entry, INFINITY for an unbounded closest-hit query),
+ * direction (not required to be normalized) and flags. */
+typedef struct pt_ray {
+    float    org[3];
+    float    tmax;
+    float    dir[3];
+    uint32_t flags;
+} pt_ray;
+#define PT_RAY_ANY_HIT 1u   /* stop at the first accepted triangle (shadow query)            */
+
+/* Result: prim = global primitive id of the committed triangle (PT_PRIM_NONE on a miss);
+ * t = final poly::Ray::MinT (= tmax on a miss); u, v = the committed barycentrics
+ * (poly::Intersection::u, v; mesh.cpp:302-303,338-339).  For an any-hit ray the fields describe
+ * the first accepted triangle. */
+typedef struct pt_hit {
+    uint32_t prim;
+    float    t;
+    float    u;
+    float    v;
+} pt_hit;
+
+#define PT_MEM_DEVICE 1u   /* rays/hits (or film) pointers are device pointers               */
+
+/* Trace n rays.  Closest-hit rays reproduce bvh::intersect_compact exactly (same node order, same
+ * Wald arithmetic, same tie-breaking); any-hit rays return whether that closest-hit query would
+ * have found any hit.  With PT_MEM_DEVICE the call is asynchronous on `stream`; with host
+ * pointers it stages through the handle's pinned buffers, overlaps the copies with the kernels
+ * and returns when the hits are on the host. */
+int pt_trace(pt_scene *scene, const pt_ray *rays, uint64_t n, pt_hit *hits,
+             uint32_t mem_flags, void *stream);
+
+/* Same traversal, also writing per-ray counts of node box tests (poly::Intersection::num_bb_hits +
+ * num_bb_misses) and triangle tests (num_triangle_isects), bvh.cpp:495,502,520.  Pointers follow
+ * mem_flags; counts may be NULL.  Used for the algorithmic-bytes accounting and order checks. */
+int pt_trace_counted(pt_scene *scene, const pt_ray *rays, uint64_t n, pt_hit *hits,
+                     uint32_t *node_tests, uint32_t *tri_tests, uint32_t mem_flags, void *stream);
+
+/* ---- rendering (the CPU render call) ----------------------------------------------------- */
+
+/* Pinhole camera as built by the PBRT "LookAt" + "Camera perspective" directives
+ * (src/common/parsers/pbrt_parser.cpp:1099-1171, Transform::LookAt Transform.cpp:322-365,
+ * PerspectiveCamera.cpp:17-49, left-handed = true). */
+typedef struct pt_camera {
+    float eye[3];
+    float look_at[3];
+    float up[3];
+    float fov_deg;
+} pt_camera;
+
+#define PT_RENDER_NEE        1u   /* area-light next-event estimation with shadow rays       */
+#define PT_RENDER_JITTER     2u   /* jittered pixel samples (default: pixel centres, the
+                                     reference CenterSampler, samplers.cpp:13-18)             */
+#define PT_RENDER_WAVEFRONT  4u   /* queue-based wavefront kernels (default: one fused path
+                                     kernel per wave)                                         */
+
+typedef struct pt_render_desc {
+    uint32_t  width, height;
+    uint32_t  spp;
+    uint32_t  max_depth;          /* PathTraceIntegrator::MaxDepth                           */
+    uint64_t  seed;               /* counter-RNG key                                         */
+    uint32_t  flags;              /* PT_RENDER_*                                             */
+    uint32_t  wave_paths;         /* paths per wave (0 = automatic)                           */
+    pt_camera camera;
+} pt_render_desc;
+
+/* Render one frame.  rgb_out: width*height*3 floats, the box-filtered film (per-sample clamp to
+ * 255 then the mean, BoxFilter.cpp:14-71) before PNG quantization.  primary_prim_out (optional):
+ * width*height global primitive ids hit by sample 0's camera ray (PT_PRIM_NONE on a miss).
+ * Pointers follow mem_flags; with host pointers the call returns when the film is on the host. */
+int pt_render(pt_scene *scene, const pt_render_desc *desc, float *rgb_out,
+              uint32_t *primary_prim_out, uint32_t mem_flags, void *stream);
+
+/* ---- synthetic workload generators (deterministic, shared by the checker and the bench) --- */
+
+/* Icosphere: icosahedron subdivided `level` times (20 * 4^level faces, 10 * 4^level + 2
+ * vertices) of the given radius, each vertex displaced radially by `noise_amp` times 3-octave
+ * seeded value noise.  Writes packed positions and faces; pass NULL to query the counts. */
+int pt_gen_icosphere(uint32_t level, float radius, float noise_amp, uint64_t noise_seed,
+                     float *x, float *y, float *z, uint32_t *num_vertices,
+                     uint32_t *fv0, uint32_t *fv1, uint32_t *fv2, uint32_t *num_faces);
+
+/* The intersection-microbench ray set: origins uniform on a sphere of radius `origin_radius`,
+ * directions normalized toward a uniform point in the unit ball; even indices are closest-hit
+ * queries (tmax = INFINITY), odd indices any-hit queries with tmax = distance to the target. */
+int pt_gen_rays(uint64_t n, float origin_radius, uint64_t seed, pt_ray *rays);
+
+/* ---- misc -------------------------------------------------------------------------------- */
+const char *pt_last_error(void);
+const char *pt_version(void);
+
+/* ---- exact-arithmetic hooks (no reference counterpart; used by the parity tests) ---------- */
+
+/* (float)((double)a*b - (double)c*d) computed without FP64 instructions, as the kernels do for
+ * the Wald test's edge fallback (src/cpu/shapes/mesh.cpp:252-264).  Host build of the same code. */
+float pt_host_f64_diff_emulated(float a, float b, float c, float d);
+
+/* Runs a device build of one exact helper over n host inputs: which = 0 f64_diff_emulated
+ * (in: 4 floats, out: 1 float per item), 1 sin/cos(2*pi*u) (in: 1 float, out: 2 floats),
+ * 2 Philox4x32-10 keyed by seed (in: 4 uint32 counters, out: 4 uint32). */
+int pt_selftest_device(int which, const void *in, void *out, uint32_t n, uint64_t seed);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* POLYTOPE_B200_H */

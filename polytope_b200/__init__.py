@@ -1,0 +1,342 @@
+"""polytope_b200 -- B200-native ray/path-tracing hot path of Polytope, behind a C ABI.
+
+This package is a thin ctypes layer over ``polytope_b200/lib/libpolytope_b200.so`` (built from
+``polytope_b200/csrc``; declared in ``include/polytope_b200.h``).  The classes mirror the
+reference's own interfaces (paths relative to the Polytope source tree):
+
+* :class:`Mesh`        -- ``poly::Mesh`` + ``poly::mesh_geometry`` (src/cpu/shapes/mesh.h:17-113)
+* :class:`Scene`       -- ``poly::Scene`` (src/cpu/scenes/Scene.h:17-35); ``Scene.intersect`` is
+  ``Scene::intersect`` (Scene.cpp:12-31) for a batch of rays
+* :func:`bvh_build`    -- ``poly::bvh::bound`` + ``compact`` (src/cpu/acceleration/bvh.cpp:36-395, 652-698)
+* :class:`GpuRunner`   -- ``poly::AbstractRunner`` (src/cpu/runners/AbstractRunner.h:38-45):
+  ``run()`` renders the frame, ``output()`` returns the film
+
+There is no CPU fallback: the library needs a CUDA device for every call that launches work, and
+importing the package fails loudly when the library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libpolytope_b200.so")
+
+PT_OK, PT_EINVAL, PT_ENOMEM, PT_ETIMEOUT, PT_ECUDA, PT_ESTACK = 0, -1, -2, -3, -4, -5
+PRIM_NONE = 0xFFFFFFFF
+MAT_LAMBERT, MAT_MIRROR = 1, 2
+RAY_ANY_HIT = 1
+MEM_DEVICE = 1
+RENDER_NEE, RENDER_JITTER, RENDER_WAVEFRONT = 1, 2, 4
+
+RAY_DTYPE = np.dtype([("org", "<f4", 3), ("tmax", "<f4"), ("dir", "<f4", 3), ("flags", "<u4")])
+HIT_DTYPE = np.dtype([("prim", "<u4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
+NODE_DTYPE = np.dtype([("bb", "<f4", 6), ("offset", "<u4"), ("num_faces", "<u2"), ("axis", "<u2")])
+
+_fp = C.POINTER(C.c_float)
+_up = C.POINTER(C.c_uint32)
+_vp = C.c_void_p
+
+
+class PolytopeError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"polytope_b200 error {code}: {msg}")
+        self.code = code
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [
+        ("x", _fp), ("y", _fp), ("z", _fp), ("num_vertices", C.c_uint32),
+        ("fv0", _up), ("fv1", _up), ("fv2", _up), ("num_faces", C.c_uint32),
+        ("nx", _fp), ("ny", _fp), ("nz", _fp),
+        ("object_to_world", C.c_float * 16), ("world_to_object", C.c_float * 16),
+        ("material", C.c_uint32), ("albedo", C.c_float * 3),
+        ("is_light", C.c_int32), ("emission", C.c_float * 3),
+    ]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("meshes", C.POINTER(MeshDesc)), ("num_meshes", C.c_uint32),
+        ("nodes", _vp), ("num_nodes", C.c_uint32), ("leaf_pairs", _up),
+        ("has_env", C.c_int32), ("env", C.c_float * 3),
+    ]
+
+
+class SceneInfo(C.Structure):
+    _fields_ = [("num_nodes", C.c_uint32), ("num_prims", C.c_uint32), ("num_meshes", C.c_uint32),
+                ("max_depth", C.c_uint32), ("device_bytes", C.c_uint64)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("eye", C.c_float * 3), ("look_at", C.c_float * 3), ("up", C.c_float * 3), ("fov_deg", C.c_float)]
+
+
+class RenderDesc(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("max_depth", C.c_uint32),
+                ("seed", C.c_uint64), ("flags", C.c_uint32), ("wave_paths", C.c_uint32), ("camera", Camera)]
+
+
+def _load() -> C.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C polytope_b200/csrc` "
+                          "(or __graft_entry__.build()); there is no CPU fallback")
+    lib = C.CDLL(LIB_PATH)
+    i, u32, u64 = C.c_int, C.c_uint32, C.c_uint64
+    sig = {
+        "pt_last_error": (C.c_char_p, []),
+        "pt_version": (C.c_char_p, []),
+        "pt_bvh_build": (i, [C.POINTER(MeshDesc), u32, i, _vp, _up, _up]),
+        "pt_scene_create": (i, [C.POINTER(SceneDesc), C.POINTER(_vp)]),
+        "pt_scene_destroy": (i, [_vp]),
+        "pt_scene_get_info": (i, [_vp, C.POINTER(SceneInfo)]),
+        "pt_trace": (i, [_vp, _vp, u64, _vp, u32, _vp]),
+        "pt_trace_counted": (i, [_vp, _vp, u64, _vp, _vp, _vp, u32, _vp]),
+        "pt_render": (i, [_vp, C.POINTER(RenderDesc), _vp, _vp, u32, _vp]),
+        "pt_gen_icosphere": (i, [u32, C.c_float, C.c_float, u64, _fp, _fp, _fp, _up, _up, _up, _up, _up]),
+        "pt_gen_rays": (i, [u64, C.c_float, u64, _vp]),
+        "pt_host_f64_diff_emulated": (C.c_float, [C.c_float] * 4),
+        "pt_selftest_device": (i, [i, _vp, _vp, u32, u64]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    return lib.pt_last_error().decode()
+
+
+def check(rc: int) -> None:
+    if rc != PT_OK:
+        raise PolytopeError(rc, last_error())
+
+
+def version() -> str:
+    return lib.pt_version().decode()
+
+
+def _f(a):
+    return a.ctypes.data_as(_fp) if a is not None else None
+
+
+def _u(a):
+    return a.ctypes.data_as(_up) if a is not None else None
+
+
+@dataclass
+class Mesh:
+    """One mesh instance (poly::Mesh): packed vertices, faces, transform, material, emission."""
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    faces: np.ndarray                      # (F, 3) uint32 vertex indices
+    object_to_world: np.ndarray = field(default_factory=lambda: np.eye(4, dtype=np.float32))
+    world_to_object: Optional[np.ndarray] = None
+    material: int = MAT_LAMBERT
+    albedo: Sequence[float] = (0.7, 0.7, 0.7)
+    is_light: bool = False
+    emission: Sequence[float] = (0.0, 0.0, 0.0)
+    normals: Optional[np.ndarray] = None   # (V, 3) packed vertex normals
+
+    def __post_init__(self):
+        self.x = np.ascontiguousarray(self.x, np.float32)
+        self.y = np.ascontiguousarray(self.y, np.float32)
+        self.z = np.ascontiguousarray(self.z, np.float32)
+        self.faces = np.ascontiguousarray(self.faces, np.uint32).reshape(-1, 3)
+        self.object_to_world = np.asarray(self.object_to_world, np.float32).reshape(4, 4)
+        if self.world_to_object is None:
+            self.world_to_object = np.linalg.inv(self.object_to_world.astype(np.float64)).astype(np.float32)
+        self.world_to_object = np.asarray(self.world_to_object, np.float32).reshape(4, 4)
+
+
+def mesh_descs(meshes: Sequence[Mesh]):
+    """ctypes array of MeshDesc (same layout as pt_mesh_desc) plus the arrays it points into."""
+    arr = (MeshDesc * len(meshes))()
+    keep = []
+    for k, m in enumerate(meshes):
+        f0, f1, f2 = (np.ascontiguousarray(m.faces[:, j]) for j in range(3))
+        keep += [m.x, m.y, m.z, f0, f1, f2]
+        d = arr[k]
+        d.x, d.y, d.z, d.num_vertices = _f(m.x), _f(m.y), _f(m.z), len(m.x)
+        d.fv0, d.fv1, d.fv2, d.num_faces = _u(f0), _u(f1), _u(f2), len(f0)
+        if m.normals is not None:
+            n = np.ascontiguousarray(m.normals, np.float32)
+            nx, ny, nz = (np.ascontiguousarray(n[:, j]) for j in range(3))
+            keep += [nx, ny, nz]
+            d.nx, d.ny, d.nz = _f(nx), _f(ny), _f(nz)
+        d.object_to_world[:] = [float(v) for v in m.object_to_world.ravel()]
+        d.world_to_object[:] = [float(v) for v in m.world_to_object.ravel()]
+        d.material = int(m.material)
+        d.albedo[:] = [float(v) for v in m.albedo]
+        d.is_light = int(bool(m.is_light))
+        d.emission[:] = [float(v) for v in m.emission]
+    return arr, keep
+
+
+def bvh_build(meshes: Sequence[Mesh], threads: int = 0):
+    """The reference SAH BVH (node-for-node identical): returns (nodes, leaf_pairs)."""
+    arr, keep = mesh_descs(meshes)
+    n = C.c_uint32(0)
+    check(lib.pt_bvh_build(arr, len(meshes), threads, None, C.byref(n), None))
+    nodes = np.zeros(n.value, NODE_DTYPE)
+    pairs = np.zeros((sum(len(m.faces) for m in meshes), 2), np.uint32)
+    check(lib.pt_bvh_build(arr, len(meshes), threads, nodes.ctypes.data, C.byref(n), _u(pairs)))
+    return nodes, pairs
+
+
+def _ptr(a) -> int:
+    """Address of a numpy array or a torch tensor (device pointers for MEM_DEVICE calls)."""
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+class Scene:
+    """poly::Scene on the GPU: meshes (Shapes and Lights), optional constant environment, BVH."""
+
+    def __init__(self, meshes: Sequence[Mesh], env: Optional[Sequence[float]] = None,
+                 nodes: Optional[np.ndarray] = None, leaf_pairs: Optional[np.ndarray] = None):
+        self.meshes = list(meshes)
+        arr, keep = mesh_descs(self.meshes)
+        d = SceneDesc()
+        d.meshes = arr
+        d.num_meshes = len(self.meshes)
+        if nodes is not None:
+            nodes = np.ascontiguousarray(nodes, NODE_DTYPE)
+            pairs = np.ascontiguousarray(leaf_pairs, np.uint32)
+            keep += [nodes, pairs]
+            d.nodes = nodes.ctypes.data
+            d.num_nodes = len(nodes)
+            d.leaf_pairs = _u(pairs)
+        d.has_env = int(env is not None)
+        if env is not None:
+            d.env[:] = [float(v) for v in env]
+        h = _vp()
+        check(lib.pt_scene_create(C.byref(d), C.byref(h)))
+        self.handle = h
+        self.prim_base = np.concatenate([[0], np.cumsum([len(m.faces) for m in self.meshes])]).astype(np.int64)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib.pt_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> SceneInfo:
+        inf = SceneInfo()
+        check(lib.pt_scene_get_info(self.handle, C.byref(inf)))
+        return inf
+
+    def intersect(self, rays, hits=None, device: bool = False, stream: int = 0, counts: bool = False):
+        """Scene::intersect for a batch: numpy (host) arrays, or torch CUDA tensors with device=True
+        (asynchronous on `stream`).  Returns hits (and node/face test counts with counts=True)."""
+        n = len(rays) if not hasattr(rays, "numel") else rays.numel() // 8
+        if hits is None:
+            if device:
+                raise ValueError("device calls need a preallocated hits tensor")
+            hits = np.zeros(n, HIT_DTYPE)
+        flags = MEM_DEVICE if device else 0
+        if not device:
+            rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        if counts:
+            if device:
+                raise ValueError("counts are host-only here")
+            nt = np.zeros(n, np.uint32)
+            tt = np.zeros(n, np.uint32)
+            check(lib.pt_trace_counted(self.handle, _ptr(rays), n, _ptr(hits), nt.ctypes.data, tt.ctypes.data, 0, None))
+            return hits, nt, tt
+        check(lib.pt_trace(self.handle, _ptr(rays), n, _ptr(hits), flags, stream or None))
+        return hits
+
+    def prim_to_mesh_face(self, prim: np.ndarray):
+        prim = np.asarray(prim, np.int64)
+        m = np.searchsorted(self.prim_base, prim, side="right") - 1
+        return m, prim - self.prim_base[m]
+
+
+def render_desc(width, height, spp, max_depth, camera, seed=1, flags=0, wave_paths=0) -> RenderDesc:
+    rd = RenderDesc()
+    rd.width, rd.height, rd.spp, rd.max_depth = width, height, spp, max_depth
+    rd.seed, rd.flags, rd.wave_paths = seed, flags, wave_paths
+    rd.camera.eye[:] = camera["eye"]
+    rd.camera.look_at[:] = camera["look_at"]
+    rd.camera.up[:] = camera["up"]
+    rd.camera.fov_deg = camera["fov"]
+    return rd
+
+
+def render(scene: Scene, width: int, height: int, spp: int, max_depth: int, camera: dict, seed: int = 1,
+           flags: int = 0, wave_paths: int = 0):
+    """One frame: returns (rgb film (H, W, 3) float32, primary prim ids (H, W) uint32)."""
+    rd = render_desc(width, height, spp, max_depth, camera, seed, flags, wave_paths)
+    rgb = np.zeros((height, width, 3), np.float32)
+    prim = np.zeros((height, width), np.uint32)
+    check(lib.pt_render(scene.handle, C.byref(rd), rgb.ctypes.data, prim.ctypes.data, 0, None))
+    return rgb, prim
+
+
+class GpuRunner:
+    """AbstractRunner shape: ``run()`` is the render call (spawn + join of the CPU runner threads),
+    ``output()`` returns the film (PNGFilm::Output minus the PNG quantization)."""
+
+    def __init__(self, scene: Scene, width: int, height: int, spp: int, max_depth: int, camera: dict,
+                 seed: int = 1, flags: int = 0):
+        self.scene, self.width, self.height, self.spp = scene, width, height, spp
+        self.max_depth, self.camera, self.seed, self.flags = max_depth, camera, seed, flags
+        self._film = None
+
+    def run(self):
+        self._film = render(self.scene, self.width, self.height, self.spp, self.max_depth, self.camera,
+                            self.seed, self.flags)
+
+    def output(self):
+        if self._film is None:
+            raise RuntimeError("run() first")
+        return self._film
+
+
+def icosphere(level: int, radius: float = 1.0, noise_amp: float = 0.0, seed: int = 0):
+    """Packed (x, y, z, faces) of the seeded displaced icosphere generator."""
+    nv, nf = C.c_uint32(0), C.c_uint32(0)
+    check(lib.pt_gen_icosphere(level, radius, noise_amp, seed, None, None, None, C.byref(nv), None, None, None, C.byref(nf)))
+    x, y, z = (np.zeros(nv.value, np.float32) for _ in range(3))
+    f0, f1, f2 = (np.zeros(nf.value, np.uint32) for _ in range(3))
+    check(lib.pt_gen_icosphere(level, radius, noise_amp, seed, _f(x), _f(y), _f(z), C.byref(nv), _u(f0), _u(f1), _u(f2), C.byref(nf)))
+    return x, y, z, np.stack([f0, f1, f2], axis=1)
+
+
+def microbench_rays(n: int, origin_radius: float = 3.0, seed: int = 11) -> np.ndarray:
+    rays = np.zeros(n, RAY_DTYPE)
+    check(lib.pt_gen_rays(n, origin_radius, seed, rays.ctypes.data))
+    return rays
+
+
+def f64_diff_emulated_host(a: float, b: float, c: float, d: float) -> float:
+    return float(lib.pt_host_f64_diff_emulated(a, b, c, d))
+
+
+def selftest_device(which: int, inp: np.ndarray, n: int, seed: int = 0) -> np.ndarray:
+    if which == 0:
+        out = np.zeros(n, np.float32)
+    elif which == 1:
+        out = np.zeros((n, 2), np.float32)
+    else:
+        out = np.zeros((n, 4), np.uint32)
+    inp = np.ascontiguousarray(inp)
+    check(lib.pt_selftest_device(which, inp.ctypes.data, out.ctypes.data, n, seed))
+    return out

@@ -1,0 +1,419 @@
+// abi.cpp -- the C ABI (include/polytope_b200.h): scene upload, ray queries, error reporting.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "exact_math.h"
+#include "launch.h"
+#include "pt_internal.h"
+
+namespace pt {
+
+namespace {
+thread_local std::string g_last_error;
+
+struct DeviceGuard {  // makes `dev` current for the scope and restores the caller's device
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail(PT_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define PT_CUDA(call)                                     \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call); \
+    } while (0)
+
+template <class T>
+int upload(void** dst, const T* src, size_t count, uint64_t& bytes) {
+    const size_t nb = sizeof(T) * count;
+    if (nb == 0) { *dst = nullptr; return PT_OK; }
+    cudaError_t e = cudaMalloc(dst, nb);
+    if (e != cudaSuccess) return fail(PT_ENOMEM, std::string("cudaMalloc scene buffer: ") + cudaGetErrorString(e));
+    bytes += nb;
+    e = cudaMemcpy(*dst, src, nb, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpy scene buffer");
+    return PT_OK;
+}
+
+void free_scene(pt_scene* s) {
+    if (!s) return;
+    DeviceGuard g(s->device);
+    void* bufs[] = {s->dev.nodes, s->dev.tris, s->dev.meshes, s->dev.prim_normals, s->dev.prim_tri,
+                    s->dev.light_tris, s->dev.light_cdf, s->dev_in, s->dev_out, s->err_flag};
+    for (void* b : bufs)
+        if (b) cudaFree(b);
+    if (s->pin_in) cudaFreeHost(s->pin_in);
+    if (s->pin_out) cudaFreeHost(s->pin_out);
+    for (void*& st : s->streams)
+        if (st) cudaStreamDestroy((cudaStream_t)st);
+    for (void*& ev : s->events)
+        if (ev) cudaEventDestroy((cudaEvent_t)ev);
+    delete s;
+}
+
+bool is_pinned(const void* p) {
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeHost;
+}
+
+constexpr size_t kChunkRays = size_t(1) << 20;
+
+int ensure_staging(pt_scene* s) {
+    if (s->staging_rays) return PT_OK;
+    for (int i = 0; i < 2; ++i) {
+        PT_CUDA(cudaStreamCreateWithFlags((cudaStream_t*)&s->streams[i], cudaStreamNonBlocking));
+    }
+    for (int i = 0; i < 4; ++i) PT_CUDA(cudaEventCreateWithFlags((cudaEvent_t*)&s->events[i], cudaEventDisableTiming));
+    const size_t in_b = 2 * kChunkRays * sizeof(pt_ray), out_b = 2 * kChunkRays * sizeof(pt_hit);
+    if (cudaMalloc(&s->dev_in, in_b) != cudaSuccess || cudaMalloc(&s->dev_out, out_b) != cudaSuccess)
+        return fail(PT_ENOMEM, "cudaMalloc staging buffers");
+    if (cudaMallocHost(&s->pin_in, in_b) != cudaSuccess || cudaMallocHost(&s->pin_out, out_b) != cudaSuccess)
+        return fail(PT_ENOMEM, "cudaMallocHost staging buffers");
+    s->staging_rays = kChunkRays;
+    return PT_OK;
+}
+
+}  // namespace
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+int scene_trace(pt_scene* s, const pt_ray* rays, uint64_t n, pt_hit* hits, uint32_t* node_tests, uint32_t* tri_tests,
+                uint32_t mem_flags, void* stream) {
+    if (!s) return fail(PT_EINVAL, "scene is NULL");
+    if (n == 0) return PT_OK;
+    if (!rays || !hits) return fail(PT_EINVAL, "rays or hits is NULL");
+    if ((int)s->max_depth + 2 > PT_TRAVERSAL_STACK)
+        return fail(PT_ESTACK, "tree depth " + std::to_string(s->max_depth) + " exceeds the traversal stack");
+    DeviceGuard g(s->device);
+    TraceArgs a{};
+    a.nodes = s->dev.nodes;
+    a.tris = s->dev.tris;
+    a.num_nodes = s->num_nodes;
+    a.err = (int*)s->err_flag;
+    if (mem_flags & PT_MEM_DEVICE) {
+        a.rays = rays;
+        a.hits = hits;
+        a.n = n;
+        a.node_tests = node_tests;
+        a.tri_tests = tri_tests;
+        cudaError_t e = launch_trace(a, (cudaStream_t)stream);
+        if (e != cudaSuccess) return cuda_fail(e, "trace kernel launch");
+        return PT_OK;
+    }
+    // Host pointers: pipeline chunks over two streams so copies overlap the kernels.
+    std::lock_guard<std::mutex> lock(s->staging_mu);
+    int rc = ensure_staging(s);
+    if (rc) return rc;
+    cudaStream_t st[2] = {(cudaStream_t)s->streams[0], (cudaStream_t)s->streams[1]};
+    cudaEvent_t done[2] = {(cudaEvent_t)s->events[0], (cudaEvent_t)s->events[1]};
+    cudaEvent_t dep = (cudaEvent_t)s->events[2];
+    PT_CUDA(cudaEventRecord(dep, (cudaStream_t)stream));
+    PT_CUDA(cudaStreamWaitEvent(st[0], dep, 0));
+    PT_CUDA(cudaStreamWaitEvent(st[1], dep, 0));
+    PT_CUDA(cudaMemsetAsync(s->err_flag, 0, sizeof(int), st[0]));
+    PT_CUDA(cudaStreamSynchronize(st[0]));
+    const bool pin_rays = is_pinned(rays), pin_hits = is_pinned(hits);
+    const bool counted = node_tests || tri_tests;
+    std::vector<uint32_t> dev_counts_host;
+    uint32_t* dcounts = nullptr;
+    if (counted) {
+        if (cudaMalloc(&dcounts, 2 * sizeof(uint32_t) * kChunkRays * 2) != cudaSuccess)
+            return fail(PT_ENOMEM, "cudaMalloc count buffers");
+    }
+    const uint64_t nchunks = (n + kChunkRays - 1) / kChunkRays;
+    uint64_t pending[2] = {~0ull, ~0ull};  // chunk whose results sit in each slot
+    auto drain = [&](int slot) -> int {
+        if (pending[slot] == ~0ull) return PT_OK;
+        PT_CUDA(cudaEventSynchronize(done[slot]));
+        const uint64_t c = pending[slot];
+        const uint64_t off = c * kChunkRays, cnt = std::min<uint64_t>(kChunkRays, n - off);
+        if (!pin_hits)
+            std::memcpy(hits + off, (pt_hit*)s->pin_out + slot * kChunkRays, cnt * sizeof(pt_hit));
+        if (counted) {
+            std::vector<uint32_t> tmp(2 * cnt);
+            PT_CUDA(cudaMemcpy(tmp.data(), dcounts + slot * 2 * kChunkRays, 2 * cnt * sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost));
+            if (node_tests) std::memcpy(node_tests + off, tmp.data(), cnt * sizeof(uint32_t));
+            if (tri_tests) std::memcpy(tri_tests + off, tmp.data() + cnt, cnt * sizeof(uint32_t));
+        }
+        pending[slot] = ~0ull;
+        return PT_OK;
+    };
+    for (uint64_t c = 0; c < nchunks; ++c) {
+        const int slot = (int)(c & 1);
+        rc = drain(slot);
+        if (rc) { if (dcounts) cudaFree(dcounts); return rc; }
+        const uint64_t off = c * kChunkRays, cnt = std::min<uint64_t>(kChunkRays, n - off);
+        pt_ray* din = (pt_ray*)s->dev_in + slot * kChunkRays;
+        pt_hit* dout = (pt_hit*)s->dev_out + slot * kChunkRays;
+        const void* src = rays + off;
+        if (!pin_rays) {
+            std::memcpy((pt_ray*)s->pin_in + slot * kChunkRays, rays + off, cnt * sizeof(pt_ray));
+            src = (pt_ray*)s->pin_in + slot * kChunkRays;
+        }
+        PT_CUDA(cudaMemcpyAsync(din, src, cnt * sizeof(pt_ray), cudaMemcpyHostToDevice, st[slot]));
+        a.rays = din;
+        a.hits = dout;
+        a.n = cnt;
+        a.node_tests = counted ? dcounts + slot * 2 * kChunkRays : nullptr;
+        a.tri_tests = counted ? dcounts + slot * 2 * kChunkRays + cnt : nullptr;
+        cudaError_t e = launch_trace(a, st[slot]);
+        if (e != cudaSuccess) { if (dcounts) cudaFree(dcounts); return cuda_fail(e, "trace kernel launch"); }
+        void* dst = pin_hits ? (void*)(hits + off) : (void*)((pt_hit*)s->pin_out + slot * kChunkRays);
+        PT_CUDA(cudaMemcpyAsync(dst, dout, cnt * sizeof(pt_hit), cudaMemcpyDeviceToHost, st[slot]));
+        PT_CUDA(cudaEventRecord(done[slot], st[slot]));
+        pending[slot] = c;
+    }
+    for (int slot = 0; slot < 2; ++slot) {
+        rc = drain(slot);
+        if (rc) { if (dcounts) cudaFree(dcounts); return rc; }
+    }
+    if (dcounts) cudaFree(dcounts);
+    int err = 0;
+    PT_CUDA(cudaMemcpy(&err, s->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return fail(PT_ESTACK, "a ray exceeded the traversal stack (malformed or too deep tree)");
+    return PT_OK;
+}
+
+}  // namespace pt
+
+using namespace pt;
+
+extern "C" {
+
+const char* pt_last_error(void) { return g_last_error.c_str(); }
+const char* pt_version(void) { return "polytope_b200 0.1 (sm_100a)"; }
+
+int pt_bvh_build(const pt_mesh_desc* meshes, uint32_t num_meshes, int threads, pt_bvh_node* nodes_out,
+                 uint32_t* num_nodes_out, uint32_t* leaf_pairs_out) {
+    if (!meshes || num_meshes == 0) return fail(PT_EINVAL, "no meshes");
+    if (!num_nodes_out) return fail(PT_EINVAL, "num_nodes_out is NULL");
+    WorldMeshes w;
+    int rc = bake_world(meshes, num_meshes, w);
+    if (rc) return rc;
+    BuiltTree t;
+    rc = build_bvh(meshes, num_meshes, w, threads, t);
+    if (rc) return rc;
+    if (!nodes_out) {
+        *num_nodes_out = (uint32_t)t.nodes.size();
+        return PT_OK;
+    }
+    if (*num_nodes_out < t.nodes.size()) return fail(PT_EINVAL, "nodes_out too small");
+    std::memcpy(nodes_out, t.nodes.data(), t.nodes.size() * sizeof(pt_bvh_node));
+    *num_nodes_out = (uint32_t)t.nodes.size();
+    if (leaf_pairs_out) std::memcpy(leaf_pairs_out, t.leaf_pairs.data(), t.leaf_pairs.size() * sizeof(uint32_t));
+    return PT_OK;
+}
+
+int pt_scene_create(const pt_scene_desc* desc, pt_scene** out) {
+    if (!desc || !out) return fail(PT_EINVAL, "desc or out is NULL");
+    *out = nullptr;
+    if (!desc->meshes || desc->num_meshes == 0) return fail(PT_EINVAL, "scene has no meshes");
+    int ndev = 0;
+    cudaError_t ce = cudaGetDeviceCount(&ndev);
+    if (ce != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(PT_ECUDA, "no CUDA device available (there is no CPU fallback)");
+    }
+    for (uint32_t m = 0; m < desc->num_meshes; ++m) {
+        const pt_mesh_desc& d = desc->meshes[m];
+        if (d.material != PT_MAT_LAMBERT && d.material != PT_MAT_MIRROR)
+            return fail(PT_EINVAL, "mesh " + std::to_string(m) + ": unknown material");
+    }
+    WorldMeshes w;
+    int rc = bake_world(desc->meshes, desc->num_meshes, w);
+    if (rc) return rc;
+    BuiltTree t;
+    if (desc->nodes) {
+        if (!desc->leaf_pairs) return fail(PT_EINVAL, "nodes given without leaf_pairs");
+        t.nodes.assign(desc->nodes, desc->nodes + desc->num_nodes);
+        t.leaf_pairs.assign(desc->leaf_pairs, desc->leaf_pairs + 2 * (size_t)w.num_prims);
+        for (size_t i = 0; i < w.num_prims; ++i) {
+            const uint32_t m = t.leaf_pairs[2 * i], f = t.leaf_pairs[2 * i + 1];
+            if (m >= desc->num_meshes || f >= desc->meshes[m].num_faces)
+                return fail(PT_EINVAL, "leaf pair " + std::to_string(i) + " out of range");
+        }
+    } else {
+        rc = build_bvh(desc->meshes, desc->num_meshes, w, 0, t);
+        if (rc) return rc;
+    }
+    uint32_t max_depth = 0;
+    rc = validate_tree(t.nodes.data(), (uint32_t)t.nodes.size(), w.num_prims, &max_depth);
+    if (rc) return rc;
+
+    std::unique_ptr<pt_scene> s(new pt_scene());
+    cudaGetDevice(&s->device);
+    s->num_nodes = (uint32_t)t.nodes.size();
+    s->num_prims = w.num_prims;
+    s->num_meshes = desc->num_meshes;
+    s->max_depth = max_depth;
+    s->prim_base = w.prim_base;
+    s->has_env = desc->has_env;
+    std::memcpy(s->env, desc->env, sizeof(s->env));
+
+    // faces in leaf order, 48 B each: {v0.xyz v1.x}{v1.yz v2.xy}{v2.z prim mesh 0}
+    std::vector<float> tris(12 * (size_t)w.num_prims);
+    for (size_t i = 0; i < w.num_prims; ++i) {
+        const uint32_t m = t.leaf_pairs[2 * i], f = t.leaf_pairs[2 * i + 1];
+        const uint32_t p = w.prim_base[m] + f;
+        const float* v = &w.tri[9 * (size_t)p];
+        float* o = &tris[12 * i];
+        std::memcpy(o, v, 9 * sizeof(float));
+        o[9] = bitsf(p);
+        o[10] = bitsf(m);
+        o[11] = 0.f;
+    }
+    // per-mesh shading records
+    std::vector<DeviceMesh> dm(desc->num_meshes);
+    bool any_normals = false;
+    for (uint32_t m = 0; m < desc->num_meshes; ++m) {
+        const pt_mesh_desc& d = desc->meshes[m];
+        dm[m].material = d.material;
+        dm[m].is_light = d.is_light ? 1 : 0;
+        std::memcpy(dm[m].albedo, d.albedo, sizeof(dm[m].albedo));
+        std::memcpy(dm[m].emission, d.emission, sizeof(dm[m].emission));
+        if (d.nx && d.ny && d.nz) any_normals = true;
+    }
+    s->has_normals = any_normals;
+    std::vector<float> normals;
+    if (any_normals) {  // world vertex normals per prim (Transform::ApplyInPlace(Normal&), mesh.cpp:388-400)
+        normals.assign(9 * (size_t)w.num_prims, 0.f);
+        for (uint32_t m = 0; m < desc->num_meshes; ++m) {
+            const pt_mesh_desc& d = desc->meshes[m];
+            if (!(d.nx && d.ny && d.nz)) continue;
+            for (uint32_t f = 0; f < d.num_faces; ++f) {
+                const uint32_t vi[3] = {d.fv0[f], d.fv1[f], d.fv2[f]};
+                float* o = &normals[9 * (size_t)(w.prim_base[m] + f)];
+                for (int k = 0; k < 3; ++k) {
+                    o[3 * k] = d.nx[vi[k]];
+                    o[3 * k + 1] = d.ny[vi[k]];
+                    o[3 * k + 2] = d.nz[vi[k]];
+                    apply_normal(d.world_to_object, &o[3 * k]);
+                }
+            }
+        }
+    }
+    // area lights (every face of an emitting mesh, mesh/face order): world triangle + CDF of
+    // 0.5 * |(v1 - v0) x (v2 - v0)|
+    std::vector<float> lt, lcdf;
+    float larea = 0.f;
+    for (uint32_t p = 0; p < w.num_prims; ++p) {
+        const uint32_t m = w.prim_mesh[p];
+        if (!desc->meshes[m].is_light) continue;
+        const float* v = &w.tri[9 * (size_t)p];
+        const float e0[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
+        const float e1[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
+        const float c[3] = {e0[1] * e1[2] - e0[2] * e1[1], e0[2] * e1[0] - e0[0] * e1[2], e0[0] * e1[1] - e0[1] * e1[0]};
+        const float area = 0.5f * std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+        larea = larea + area;
+        for (int k = 0; k < 9; ++k) lt.push_back(v[k]);
+        lt.push_back(bitsf(p));
+        lt.push_back(bitsf(m));
+        lt.push_back(0.f);
+        lt.push_back(0.f);
+        lcdf.push_back(larea);
+    }
+    s->dev.num_lights = (uint32_t)lcdf.size();
+    s->dev.light_area = larea;
+
+    DeviceGuard g(s->device);
+    uint64_t bytes = 0;
+    if ((rc = upload(&s->dev.nodes, t.nodes.data(), t.nodes.size(), bytes))) { free_scene(s.release()); return rc; }
+    if ((rc = upload(&s->dev.tris, tris.data(), tris.size(), bytes))) { free_scene(s.release()); return rc; }
+    if ((rc = upload(&s->dev.meshes, dm.data(), dm.size(), bytes))) { free_scene(s.release()); return rc; }
+    if ((rc = upload(&s->dev.prim_tri, w.tri.data(), w.tri.size(), bytes))) { free_scene(s.release()); return rc; }
+    if (any_normals && (rc = upload(&s->dev.prim_normals, normals.data(), normals.size(), bytes))) { free_scene(s.release()); return rc; }
+    if (!lt.empty()) {
+        if ((rc = upload(&s->dev.light_tris, lt.data(), lt.size(), bytes))) { free_scene(s.release()); return rc; }
+        if ((rc = upload(&s->dev.light_cdf, lcdf.data(), lcdf.size(), bytes))) { free_scene(s.release()); return rc; }
+    }
+    if (cudaMalloc(&s->err_flag, sizeof(int)) != cudaSuccess) { free_scene(s.release()); return fail(PT_ENOMEM, "cudaMalloc error flag"); }
+    cudaMemset(s->err_flag, 0, sizeof(int));
+    s->device_bytes = bytes;
+    *out = s.release();
+    return PT_OK;
+}
+
+int pt_scene_destroy(pt_scene* scene) {
+    if (!scene) return PT_OK;
+    free_scene(scene);
+    return PT_OK;
+}
+
+int pt_scene_get_info(const pt_scene* s, pt_scene_info* info) {
+    if (!s || !info) return fail(PT_EINVAL, "scene or info is NULL");
+    info->num_nodes = s->num_nodes;
+    info->num_prims = s->num_prims;
+    info->num_meshes = s->num_meshes;
+    info->max_depth = s->max_depth;
+    info->device_bytes = s->device_bytes;
+    return PT_OK;
+}
+
+int pt_trace(pt_scene* scene, const pt_ray* rays, uint64_t n, pt_hit* hits, uint32_t mem_flags, void* stream) {
+    return scene_trace(scene, rays, n, hits, nullptr, nullptr, mem_flags, stream);
+}
+
+int pt_trace_counted(pt_scene* scene, const pt_ray* rays, uint64_t n, pt_hit* hits, uint32_t* node_tests,
+                     uint32_t* tri_tests, uint32_t mem_flags, void* stream) {
+    if (!node_tests && !tri_tests) return fail(PT_EINVAL, "no count outputs");
+    return scene_trace(scene, rays, n, hits, node_tests, tri_tests, mem_flags, stream);
+}
+
+// ---- exact-arithmetic hooks for the parity tests ------------------------------------------------
+
+float pt_host_f64_diff_emulated(float a, float b, float c, float d) { return f64_diff_emulated(a, b, c, d); }
+
+int pt_selftest_device(int which, const void* in, void* out, uint32_t n, uint64_t seed) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(PT_ECUDA, "no CUDA device available");
+    }
+    const size_t in_b = (which == 1) ? 4 * n : 16 * (size_t)n;
+    const size_t out_b = (which == 0) ? 4 * (size_t)n : (which == 1 ? 8 * (size_t)n : 16 * (size_t)n);
+    void *din = nullptr, *dout = nullptr;
+    if (cudaMalloc(&din, in_b) != cudaSuccess || cudaMalloc(&dout, out_b) != cudaSuccess) {
+        if (din) cudaFree(din);
+        return fail(PT_ENOMEM, "cudaMalloc selftest");
+    }
+    cudaMemcpy(din, in, in_b, cudaMemcpyHostToDevice);
+    cudaError_t e;
+    if (which == 0) e = launch_selftest_f64((const float*)din, (float*)dout, n, 0);
+    else if (which == 1) e = launch_selftest_sincos((const float*)din, (float*)dout, n, 0);
+    else e = launch_selftest_philox((const uint32_t*)din, (uint32_t*)dout, n, seed, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, out_b, cudaMemcpyDeviceToHost);
+    cudaFree(din);
+    cudaFree(dout);
+    if (e != cudaSuccess) return cuda_fail(e, "selftest");
+    return PT_OK;
+}
+
+}  // extern "C"

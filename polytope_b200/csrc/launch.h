@@ -1,0 +1,29 @@
+// launch.h -- host-callable launchers implemented in the .cu translation units.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace pt {
+
+struct TraceArgs {
+    const void* nodes;     // uint4 x 2 per node
+    const void* tris;      // float4 x 3 per leaf-ordered face
+    uint32_t num_nodes;
+    const void* rays;      // float4 x 2 per ray
+    void* hits;            // uint4 per ray
+    uint64_t n;
+    uint32_t* node_tests;  // optional
+    uint32_t* tri_tests;   // optional
+    int* err;              // device flag, set to 1 when a ray overflowed its stack
+};
+
+cudaError_t launch_trace(const TraceArgs& a, cudaStream_t s);
+
+// Device self-tests of the exact-arithmetic helpers (used by the GPU parity tests).
+cudaError_t launch_selftest_f64(const float* in4, float* out, uint32_t n, cudaStream_t s);
+cudaError_t launch_selftest_sincos(const float* u, float* out2, uint32_t n, cudaStream_t s);
+cudaError_t launch_selftest_philox(const uint32_t* in4, uint32_t* out4, uint32_t n, uint64_t seed, cudaStream_t s);
+
+}  // namespace pt

@@ -1,0 +1,94 @@
+// pt_internal.h -- host-side internals shared by the C++ and CUDA translation units.
+#pragma once
+
+#include <cstdint>
+#include <cstddef>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/polytope_b200.h"
+#include "config.h"
+
+namespace pt {
+
+// ---- error state ------------------------------------------------------------------------------
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);  // sets the message, returns code
+
+// ---- host BVH build (identical to the reference) ------------------------------------------------
+struct WorldMeshes {
+    // world-space triangle of each global primitive id (9 floats), owning mesh and face
+    std::vector<float> tri;        // 9 * num_prims
+    std::vector<uint32_t> prim_mesh;
+    std::vector<uint32_t> prim_base;  // per mesh
+    uint32_t num_prims = 0;
+};
+
+// Applies each mesh's object_to_world to its packed vertices exactly as
+// Transform::ApplyInPlace(Point&) does (Transform.cpp:69-91).
+void apply_point(const float* m, float p[3]);
+void apply_normal(const float* inv, float n[3]);
+int bake_world(const pt_mesh_desc* meshes, uint32_t num_meshes, WorldMeshes& out);
+
+struct BuiltTree {
+    std::vector<pt_bvh_node> nodes;
+    std::vector<uint32_t> leaf_pairs;  // 2 per leaf-ordered entry: (mesh, face)
+    uint32_t max_depth = 0;
+};
+int build_bvh(const pt_mesh_desc* meshes, uint32_t num_meshes, const WorldMeshes& w, int threads, BuiltTree& out);
+
+// Ray queries behind pt_trace / pt_trace_counted (abi.cpp).
+int scene_trace(pt_scene* s, const pt_ray* rays, uint64_t n, pt_hit* hits, uint32_t* node_tests,
+                uint32_t* tri_tests, uint32_t mem_flags, void* stream);
+
+// Checks that every child / leaf range stays inside the arrays and computes the deepest level.
+int validate_tree(const pt_bvh_node* nodes, uint32_t num_nodes, uint32_t num_leaf_entries, uint32_t* max_depth);
+
+// ---- device scene -------------------------------------------------------------------------------
+struct DeviceMesh {  // per-mesh shading record (device)
+    uint32_t material;
+    int32_t is_light;
+    float albedo[3];
+    float emission[3];
+};
+
+struct SceneDev {
+    // traversal data
+    void* nodes = nullptr;        // num_nodes * 32 B  (pt_bvh_node)
+    void* tris = nullptr;         // num_prims * 48 B  (3 x float4 per leaf-ordered entry)
+    // shading data
+    void* meshes = nullptr;       // num_meshes * DeviceMesh
+    void* prim_normals = nullptr; // num_prims * 9 floats (world vertex normals by prim id) or null
+    void* prim_tri = nullptr;     // num_prims * 9 floats world triangle by prim id
+    void* light_tris = nullptr;   // num_lights * 12 floats: v0, v1, v2, then (prim, mesh, 0, 0)
+    void* light_cdf = nullptr;    // num_lights floats
+    uint32_t num_lights = 0;
+    float light_area = 0.f;
+};
+
+}  // namespace pt
+
+struct pt_scene {
+    pt::SceneDev dev;
+    uint32_t num_nodes = 0;
+    uint32_t num_prims = 0;
+    uint32_t num_meshes = 0;
+    uint32_t max_depth = 0;
+    uint64_t device_bytes = 0;
+    int device = 0;
+    int has_env = 0;
+    float env[3] = {0.f, 0.f, 0.f};
+    bool has_normals = false;
+    std::vector<uint32_t> prim_base;
+    // staging for host-pointer calls (lazily allocated, guarded by staging_mu)
+    std::mutex staging_mu;
+    void* pin_in = nullptr;
+    void* pin_out = nullptr;
+    void* dev_in = nullptr;
+    void* dev_out = nullptr;
+    size_t staging_rays = 0;
+    void* streams[2] = {nullptr, nullptr};
+    void* events[4] = {nullptr, nullptr, nullptr, nullptr};
+    void* err_flag = nullptr;  // device int, set when a kernel hit a guard
+};

@@ -1,0 +1,212 @@
+// traverse.cuh -- device traversal of the reference BVH (closest-hit and any-hit).
+//
+// Reference semantics reproduced exactly (paths relative to the Polytope source tree):
+//   bvh::intersect_compact           src/cpu/acceleration/bvh.cpp:476-523
+//     - ordered DFS; a node's own box is tested when it is popped, against the running MinT
+//     - interior: if the ray's inverse direction is negative on the node's split axis the low
+//       child is pushed first (so the high child pops first), else the high child first
+//     - leaf: every face in leaf order goes through the Wald test
+//   BoundingBox::Hits                src/cpu/structures/BoundingBox.cpp:12-85
+//   Mesh::intersect Wald core        src/cpu/shapes/mesh.cpp:196-340
+// Ties are "last accepted wins" because a later face with the same t passes `T > MinT*det`.
+//
+// Data layout in HBM (all read with 128-bit non-coherent loads):
+//   nodes  32 B  {bb_min.xyz, bb_max.xyz, offset, num_faces | axis << 16}   (2 x uint4)
+//   tris   48 B  {v0.xyz v1.x}{v1.yz v2.xy}{v2.z prim mesh 0} in leaf order (3 x float4)
+//   rays   32 B  {org.xyz tmax}{dir.xyz flags}                              (2 x float4)
+//   hits   16 B  {prim t u v}                                              (1 x uint4)
+#pragma once
+
+#include <cstdint>
+
+#include "config.h"
+#include "exact_math.h"
+
+namespace pt {
+
+constexpr uint32_t kPrimNone = 0xFFFFFFFFu;
+constexpr int kStackCap = PT_TRAVERSAL_STACK;
+
+struct RayState {
+    float ox, oy, oz;
+    float dx, dy, dz;
+    float ix, iy, iz;          // 1/d (bvh.cpp:477-481)
+    int kx, ky, kz;            // Wald axis permutation (mesh.cpp:196-211)
+    float sx, sy, sz;          // shear constants (mesh.cpp:234-236)
+    float okx, oky, okz;       // permuted origin
+    float dkx, dky, dkz;
+};
+
+__device__ __forceinline__ float sel3(int k, float x, float y, float z) { return k == 0 ? x : (k == 1 ? y : z); }
+
+__device__ __forceinline__ void ray_setup(RayState& r, float ox, float oy, float oz, float dx, float dy, float dz) {
+    r.ox = ox; r.oy = oy; r.oz = oz;
+    r.dx = dx; r.dy = dy; r.dz = dz;
+    r.ix = frcp(dx); r.iy = frcp(dy); r.iz = frcp(dz);
+    const float ax = fabs_(dx), ay = fabs_(dy), az = fabs_(dz);
+    int kz = 0;
+    if (ay > ax && ay > az) kz = 1;
+    else if (az > ax && az > ay) kz = 2;
+    int kx = kz + 1; if (kx == 3) kx = 0;
+    int ky = kx + 1; if (ky == 3) ky = 0;
+    r.kx = kx; r.ky = ky; r.kz = kz;
+    r.dkx = sel3(kx, dx, dy, dz); r.dky = sel3(ky, dx, dy, dz); r.dkz = sel3(kz, dx, dy, dz);
+    r.okx = sel3(kx, ox, oy, oz); r.oky = sel3(ky, ox, oy, oz); r.okz = sel3(kz, ox, oy, oz);
+    r.sx = fdiv(-r.dkx, r.dkz);
+    r.sy = fdiv(-r.dky, r.dkz);
+    r.sz = frcp(r.dkz);
+}
+
+// BoundingBox::Hits with the running MinT as the far bound.
+__device__ __forceinline__ bool box_hits(const RayState& r, float b0, float b1, float b2, float b3, float b4, float b5,
+                                         float min_t) {
+    const bool inside = r.ox > b0 && r.ox < b3 && r.oy > b1 && r.oy < b4 && r.oz > b2 && r.oz < b5;
+    if (inside) return true;
+    const float gm = bitsf(PT_GAMMA_MUL_BITS);
+    float far_t = min_t, near_t = 0.f;
+    float tn = fmul(fsub(b0, r.ox), r.ix), tf = fmul(fsub(b3, r.ox), r.ix);
+    float sw = tn;
+    tn = tn > tf ? tf : tn;
+    tf = sw > tf ? sw : tf;
+    tf = fmul(tf, gm);
+    near_t = (tn > near_t) ? tn : near_t;
+    far_t = (tf < far_t) ? tf : far_t;
+    if (near_t > far_t) return false;
+    tn = fmul(fsub(b1, r.oy), r.iy); tf = fmul(fsub(b4, r.oy), r.iy);
+    sw = tn;
+    tn = tn > tf ? tf : tn;
+    tf = sw > tf ? sw : tf;
+    tf = fmul(tf, gm);
+    near_t = (tn > near_t) ? tn : near_t;
+    far_t = (tf < far_t) ? tf : far_t;
+    if (near_t > far_t) return false;
+    tn = fmul(fsub(b2, r.oz), r.iz); tf = fmul(fsub(b5, r.oz), r.iz);
+    sw = tn;
+    tn = tn > tf ? tf : tn;
+    tf = sw > tf ? sw : tf;
+    tf = fmul(tf, gm);
+    near_t = (tn > near_t) ? tn : near_t;
+    far_t = (tf < far_t) ? tf : far_t;
+    return near_t <= far_t;
+}
+
+__device__ __forceinline__ float max3abs(float x, float y, float z) {  // max_component(abs(v)), mesh.cpp:145-155
+    x = fabs_(x); y = fabs_(y); z = fabs_(z);
+    if (x >= y && x >= z) return x;
+    if (y >= x && y >= z) return y;
+    return z;
+}
+
+// One face of Mesh::intersect (mesh.cpp:196-322).  Vertices are world space.
+__device__ __forceinline__ bool wald(const RayState& r, float v0x, float v0y, float v0z, float v1x, float v1y,
+                                     float v1z, float v2x, float v2y, float v2z, float min_t, float& t_out,
+                                     float& u_out, float& v_out, float& w_out) {
+    // p_it = permute(v_i - O)
+    float p0x = fsub(sel3(r.kx, v0x, v0y, v0z), r.okx), p0y = fsub(sel3(r.ky, v0x, v0y, v0z), r.oky),
+          p0z = fsub(sel3(r.kz, v0x, v0y, v0z), r.okz);
+    float p1x = fsub(sel3(r.kx, v1x, v1y, v1z), r.okx), p1y = fsub(sel3(r.ky, v1x, v1y, v1z), r.oky),
+          p1z = fsub(sel3(r.kz, v1x, v1y, v1z), r.okz);
+    float p2x = fsub(sel3(r.kx, v2x, v2y, v2z), r.okx), p2y = fsub(sel3(r.ky, v2x, v2y, v2z), r.oky),
+          p2z = fsub(sel3(r.kz, v2x, v2y, v2z), r.okz);
+    p0x = ffma(r.sx, p0z, p0x); p0y = ffma(r.sy, p0z, p0y);
+    p1x = ffma(r.sx, p1z, p1x); p1y = ffma(r.sy, p1z, p1y);
+    p2x = ffma(r.sx, p2z, p2x); p2y = ffma(r.sy, p2z, p2y);
+    float U = diff_prod(p1x, p2y, p1y, p2x);
+    float V = diff_prod(p2x, p0y, p2y, p0x);
+    float W = diff_prod(p0x, p1y, p0y, p1x);
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {  // mesh.cpp:252-264, without FP64 instructions
+        U = f64_diff_emulated(p2y, p1x, p2x, p1y);
+        V = f64_diff_emulated(p0y, p2x, p0x, p2y);
+        W = f64_diff_emulated(p1y, p0x, p1x, p0y);
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    const float det = fadd(fadd(U, V), W);
+    if (det == 0.0f) return false;
+    p0z = fmul(p0z, r.sz); p1z = fmul(p1z, r.sz); p2z = fmul(p2z, r.sz);
+    const float T = ffma(U, p0z, sum_prod(V, p1z, W, p2z));
+    const float md = fmul(min_t, det);
+    if (det < 0.f && (T >= 0 || T < md)) return false;
+    if (det > 0.f && (T <= 0 || T > md)) return false;
+    const float rcp = frcp(det);
+    const float t = fmul(T, rcp);
+    const float g2 = bitsf(PT_GAMMA2_BITS), g3 = bitsf(PT_GAMMA3_BITS), g5 = bitsf(PT_GAMMA5_BITS);
+    const float max_zt = max3abs(p0z, p1z, p2z);
+    const float delta_z = fmul(g3, max_zt);
+    const float max_xt = max3abs(p0x, p1x, p2x);
+    const float max_yt = max3abs(p0y, p1y, p2y);
+    const float delta_x = fmul(g5, fadd(max_xt, max_zt));
+    const float delta_y = fmul(g5, fadd(max_yt, max_zt));
+    const float delta_e = fmul(2.0f, fadd(fadd(fmul(fmul(g2, max_xt), max_yt), fmul(delta_y, max_xt)), fmul(delta_x, max_yt)));
+    const float max_e = max3abs(U, V, W);
+    const float delta_t = fmul(fmul(3.0f, fadd(fadd(fmul(fmul(g3, max_e), max_zt), fmul(delta_e, max_zt)), fmul(delta_z, max_e))),
+                               fabs_(rcp));
+    if (t <= delta_t) return false;
+    t_out = t;
+    u_out = fmul(U, rcp);
+    v_out = fmul(V, rcp);
+    w_out = fmul(W, rcp);
+    return true;
+}
+
+struct TraceResult {
+    uint32_t prim;   // global primitive id or kPrimNone
+    uint32_t leaf;   // leaf-ordered index of the committed face
+    float t, u, v, w;
+    uint32_t nodes, tris;
+    bool overflow;
+};
+
+// bvh::intersect_compact.  `any` stops at the first accepted face.  COUNT keeps the per-ray node
+// and face test counts (Intersection::num_bb_hits + num_bb_misses, num_triangle_isects).
+template <bool COUNT>
+__device__ __forceinline__ TraceResult traverse(const uint4* __restrict__ nodes, const float4* __restrict__ tris,
+                                                uint32_t num_nodes, const RayState& r, float tmax, bool any) {
+    TraceResult res;
+    res.prim = kPrimNone;
+    res.leaf = kPrimNone;
+    res.t = tmax;
+    res.u = res.v = res.w = 0.f;
+    res.nodes = res.tris = 0;
+    res.overflow = false;
+    const bool neg_x = r.ix < 0, neg_y = r.iy < 0, neg_z = r.iz < 0;
+    uint32_t stack[kStackCap];
+    int sp = 0;
+    stack[sp++] = 0;
+    float min_t = tmax;
+    while (sp > 0) {
+        const uint32_t ni = stack[--sp];
+        if (ni >= num_nodes) { res.overflow = true; break; }  // malformed tree guard
+        const uint4 a = __ldg(nodes + 2 * (size_t)ni);
+        const uint4 b = __ldg(nodes + 2 * (size_t)ni + 1);
+        if (COUNT) res.nodes++;
+        if (!box_hits(r, __uint_as_float(a.x), __uint_as_float(a.y), __uint_as_float(a.z), __uint_as_float(a.w),
+                      __uint_as_float(b.x), __uint_as_float(b.y), min_t))
+            continue;
+        const uint32_t nf = b.w & 0xFFFFu;
+        if (nf > 0) {
+            for (uint32_t k = 0; k < nf; ++k) {
+                const size_t ti = 3 * (size_t)(b.z + k);
+                const float4 q0 = __ldg(tris + ti), q1 = __ldg(tris + ti + 1), q2 = __ldg(tris + ti + 2);
+                if (COUNT) res.tris++;
+                float t, u, v, w;
+                if (wald(r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, min_t, t, u, v, w)) {
+                    min_t = t;
+                    res.prim = __float_as_uint(q2.y);
+                    res.leaf = b.z + k;
+                    res.t = t; res.u = u; res.v = v; res.w = w;
+                    if (any) return res;
+                }
+            }
+            continue;
+        }
+        if (sp + 2 > kStackCap) { res.overflow = true; break; }
+        const uint32_t axis = b.w >> 16;
+        const bool neg = axis == 0 ? neg_x : (axis == 1 ? neg_y : neg_z);
+        const uint32_t hi = ni + b.z, lo = ni + 1;
+        stack[sp++] = neg ? lo : hi;
+        stack[sp++] = neg ? hi : lo;
+    }
+    return res;
+}
+
+}  // namespace pt

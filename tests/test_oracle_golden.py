@@ -1,0 +1,208 @@
+"""The CPU oracle (oracle/oracle.cpp) against the reference's own unit-test vectors and against
+fixtures produced by running the reference's code (tests/golden/make_golden.py)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, assert_bit_equal, load_golden
+from oracle import pyoracle as po
+import polytope_b200 as pb
+from polytope_b200 import workloads as W
+from golden.make_golden import scene_inputs_digest, sha  # noqa: E402
+
+CASES = json.load(open(os.path.join(GOLDEN, "reference_unit_cases.json")))
+ULP4 = 4
+
+
+def ulps(a, b):
+    a, b = np.float32(a), np.float32(b)
+    ia, ib = int(a.view(np.int32)), int(b.view(np.int32))
+    if ia < 0:
+        ia = -0x80000000 - ia
+    if ib < 0:
+        ib = -0x80000000 - ib
+    return abs(ia - ib)
+
+
+def one_triangle_mesh(verts, f):
+    v = np.asarray(verts, np.float32)
+    return pb.Mesh(v[:, 0], v[:, 1], v[:, 2], np.asarray([f], np.uint32))
+
+
+def single_ray(o, d, tmax=np.inf, flags=0):
+    r = np.zeros(1, po.RAY_DTYPE)
+    r["org"] = o
+    r["dir"] = d
+    r["tmax"] = tmax
+    r["flags"] = flags
+    return r
+
+
+def test_mesh_one_triangle_both_windings():
+    c = CASES["mesh_one_triangle"]
+    for f0, f1, f2, oz, dz, nz in c["cases"]:
+        s = po.OracleScene([one_triangle_mesh(c["vertices"], (f0, f1, f2))])
+        ray = single_ray((0.2, 0.2, oz), (0, 0, dz))
+        hit = s.trace(ray)[0]
+        assert hit["prim"] == 0
+        fr = s.hit_frames(ray)[0]
+        loc, n = fr[0:3], fr[3:6]
+        assert tuple(n) == (0.0, 0.0, float(nz)) or (ulps(n[0], 0) <= ULP4 and ulps(n[1], 0) <= ULP4 and ulps(n[2], nz) <= ULP4)
+        for k in range(3):
+            assert ulps(loc[k], c["expected_location"][k]) <= ULP4, (loc, f0, f1, f2)
+
+
+def test_mesh_stay_above_surface():
+    from golden.make_golden import stay_above_mesh, stay_above_rays
+    c = CASES["mesh_stay_above_surface"]
+    s = po.OracleScene([stay_above_mesh(c)])
+    rays = stay_above_rays(c, c["k_values"])
+    assert (s.trace(rays)["prim"] == 0).all()
+    for fr in s.hit_frames(rays):
+        for j in range(3):
+            assert ulps(fr[3 + j], c["expected_normal"][j]) <= ULP4, fr[3:6]
+        # The reference test compares Location.z with 0.2 only at k = 9999999, a ray its own
+        # Wald test rejects; the compiled reference's spawn point sits 6-8 ulps below the plane
+        # (the robust offset toward the incoming side, mesh.cpp:419-436).
+        assert ulps(fr[2], c["expected_location_z"]) <= 16, fr[0:3]
+    # farther rays: the compiled reference rejects them, so must the restatement
+    assert (s.trace(stay_above_rays(c, c["k_values_reference_misses"]))["prim"] == po.PRIM_NONE).all()
+
+
+def test_bvh_compact_offsets():
+    for name, t in CASES["bvh_compact"]["trees"].items():
+        got = po.compact_shape(t["low"], t["high"])
+        assert [g[0] for g in got] == t["expect_tags"], name
+        for idx, off in t["expect_offsets"].items():
+            assert got[int(idx)][1] == off, (name, idx, got)
+
+
+def test_bvh_bound_root_and_split():
+    c = CASES["bvh_bound"]
+    s = po.OracleScene([one_triangle_mesh(c["one_triangle"], (0, 1, 2))])
+    nodes, _ = s.tree()
+    assert len(nodes) == 1 and nodes[0]["num_faces"] == 1
+    off = c["four_triangles_offset"]
+    v = np.array([[0 + i * off, 0, 0] for i in range(4)] + [[1 + i * off, 0, 0] for i in range(4)] +
+                 [[0 + i * off, 1, 0] for i in range(4)], np.float32)
+    faces = np.array([[i, 4 + i, 8 + i] for i in range(4)], np.uint32)
+    s = po.OracleScene([pb.Mesh(v[:, 0], v[:, 1], v[:, 2], faces)])
+    nodes, _ = s.tree()
+    assert nodes[0]["num_faces"] == 0 and len(nodes) >= 3  # root split into low and high children
+
+
+def test_bbox_hits_cases():
+    for bmin, bmax, o, d, exp in CASES["bbox_hits"]["cases"]:
+        assert po.bbox_hits("orc", bmin + bmax, o, d) == exp, (bmin, bmax, o, d)
+
+
+def test_world_to_local_and_mirror():
+    for n, t1, t2, w, exp in CASES["world_to_local"]["cases"]:
+        got = po.world_to_local(t1, n, t2, w)
+        assert tuple(got) == tuple(np.float32(exp)), (got, exp)
+    for inc, exp in CASES["mirror_sample"]["cases"]:
+        got = po.mirror_sample(po.normalize(inc))
+        assert_bit_equal(got, po.normalize(exp), "mirror")
+
+
+def test_philox_known_answers():
+    for ctr, key, exp in CASES["philox4x32_10_kat"]["cases"]:
+        c = [int(x, 16) for x in ctr]
+        k = [int(x, 16) for x in key]
+        got = po.philox(c, k[0] | (k[1] << 32))
+        assert [int(x) for x in got] == [int(x, 16) for x in exp]
+
+
+def test_small_scene_fixture():
+    g = load_golden("small_scene.npz")
+    meshes, env = W.small_scene()
+    assert scene_inputs_digest(meshes) == str(g["inputs_sha"])
+    s = po.OracleScene(meshes, env)
+    nodes, pairs = s.tree()
+    assert len(nodes) == int(g["num_nodes"]) and sha(nodes, pairs) == str(g["tree_sha"])
+    hits, nt, tt = s.trace(g["rays"], counts=True)
+    closest = g["rays"]["flags"] == 0
+    for f in ("prim", "t", "u", "v"):
+        assert_bit_equal(hits[f][closest], g["hits"][f][closest], f)
+    assert_bit_equal((hits["prim"] != po.PRIM_NONE)[~closest], (g["hits"]["prim"] != po.PRIM_NONE)[~closest], "any")
+    assert_bit_equal(nt[closest], g["node_tests"][closest], "node tests")
+    assert_bit_equal(tt[closest], g["tri_tests"][closest], "tri tests")
+    rays_c = g["rays"][closest][:2048]
+    assert_bit_equal(s.hit_frames(rays_c), g["frames"], "frames")
+
+
+def test_small_scene_camera_and_render_fixture():
+    g = load_golden("small_scene.npz")
+    meshes, env = W.small_scene()
+    s = po.OracleScene(meshes, env)
+    small = dict(width=80, height=60, spp=4, max_depth=4, seed=1, camera=W.SMALL_CAMERA)
+    assert_bit_equal(po.camera_rays_oracle(small).view(np.uint32), g["camera_rays"].view(np.uint32), "camera")
+    for flags, key in ((1, "nee"), (0, "bsdf")):
+        rgb, prim = s.render(dict(small, flags=flags))
+        assert_bit_equal(rgb, g[f"rgb_{key}"], f"rgb {key}")
+        assert_bit_equal(prim, g[f"prim_{key}"], f"prim {key}")
+    assert g["rgb_nee"].mean() > 0
+
+
+def test_microbench_fixture():
+    g = load_golden("microbench.npz")
+    mm, rays = W.microbench(n_rays=65536)
+    assert scene_inputs_digest(mm) == str(g["inputs_sha"]) and sha(rays) == str(g["rays_sha"])
+    s = po.OracleScene(mm)
+    nodes, pairs = s.tree()
+    assert sha(nodes, pairs) == str(g["tree_sha"])
+    hits, nt, tt = s.trace(rays, counts=True)
+    closest = rays["flags"] == 0
+    for f in ("prim", "t", "u", "v"):
+        assert_bit_equal(hits[f][closest], g["hits"][f][closest], f)
+    assert_bit_equal((hits["prim"] != po.PRIM_NONE)[~closest], (g["hits"]["prim"] != po.PRIM_NONE)[~closest], "any")
+    assert_bit_equal(nt[closest], g["node_tests"][closest], "nodes")
+    assert_bit_equal(tt[closest], g["tri_tests"][closest], "tris")
+
+
+def test_instanced_fixture():
+    g = load_golden("instanced_small.npz")
+    im, env = W.instanced_scene(level=4)
+    assert scene_inputs_digest(im) == str(g["inputs_sha"])
+    s = po.OracleScene(im, env)
+    nodes, pairs = s.tree()
+    assert sha(nodes, pairs) == str(g["tree_sha"])
+    rgb, prim = s.render(dict(width=64, height=40, spp=2, max_depth=8, seed=1, camera=W.INSTANCED_CAMERA, flags=1))
+    assert_bit_equal(rgb, g["rgb"], "rgb")
+    assert_bit_equal(prim, g["prim"], "prim")
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="oracle/_ref is only built where the reference tree is present")
+def test_oracle_matches_reference_on_random_multimesh_scene():
+    rng = np.random.default_rng(7)
+    meshes = []
+    for k in range(3):
+        c = rng.uniform(-3, 3, (1500, 3)).astype(np.float32)
+        v = (c[:, None, :] + rng.normal(0, 0.2, (1500, 3, 3))).astype(np.float32).reshape(-1, 3)
+        M = np.eye(4, dtype=np.float32)
+        M[:3, 3] = rng.uniform(-1, 1, 3)
+        M[0, 1] = 0.25 * k
+        meshes.append(pb.Mesh(v[:, 0], v[:, 1], v[:, 2], np.arange(4500, dtype=np.uint32).reshape(-1, 3),
+                              object_to_world=M, material=1 + (k % 2), is_light=(k == 2), emission=(900,) * 3 if k == 2 else (0,) * 3))
+    o, r = po.OracleScene(meshes, (30, 40, 50)), po.RefScene(meshes, (30, 40, 50))
+    no, po_ = o.tree()
+    nr, pr = r.tree()
+    assert no.tobytes() == nr.tobytes() and (po_ == pr).all()
+    from golden.make_golden import random_rays
+    rays = random_rays(20000, 3, anyhit_tmax=2.5)
+    ho, nto, tto = o.trace(rays, counts=True)
+    hr, ntr, ttr = r.trace(rays, counts=True)
+    c = rays["flags"] == 0
+    for f in ("prim", "t", "u", "v"):
+        assert_bit_equal(ho[f][c], hr[f][c], f)
+    assert_bit_equal(nto[c], ntr[c], "nodes")
+    assert ((ho["prim"] != po.PRIM_NONE) == (hr["prim"] != po.PRIM_NONE)).all()
+    assert_bit_equal(o.hit_frames(rays[c][:3000]), r.hit_frames(rays[c][:3000]), "frames")
+    desc = dict(width=40, height=30, spp=3, max_depth=5, seed=9, flags=3,
+                camera=dict(eye=(0, 1, 9), look_at=(0, 0, 0), up=(0, 1, 0), fov=50.0))
+    a, pa = o.render(desc)
+    b, pb_ = r.render(desc)
+    assert_bit_equal(a, b, "render")
+    assert_bit_equal(pa, pb_, "prim")
