@@ -58,7 +58,7 @@ void free_scene(pt_scene* s) {
     if (!s) return;
     DeviceGuard g(s->device);
     void* bufs[] = {s->dev.nodes, s->dev.tris, s->dev.meshes, s->dev.prim_normals, s->dev.prim_tri,
-                    s->dev.light_tris, s->dev.light_cdf, s->dev_in, s->dev_out, s->err_flag};
+                    s->dev.light_tris, s->dev.light_cdf, s->dev_in, s->dev_out, s->err_flag, s->ray_counters};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (s->pin_in) cudaFreeHost(s->pin_in);
@@ -117,7 +117,11 @@ int scene_trace(pt_scene* s, const pt_ray* rays, uint64_t n, pt_hit* hits, uint3
     a.tris = s->dev.tris;
     a.num_nodes = s->num_nodes;
     a.err = (int*)s->err_flag;
+    auto next_counter = [s]() {
+        return (void*)((unsigned long long*)s->ray_counters + (s->counter_next.fetch_add(1) % PT_RAY_COUNTERS));
+    };
     if (mem_flags & PT_MEM_DEVICE) {
+        a.counter = next_counter();
         a.rays = rays;
         a.hits = hits;
         a.n = n;
@@ -182,6 +186,7 @@ int scene_trace(pt_scene* s, const pt_ray* rays, uint64_t n, pt_hit* hits, uint3
         a.rays = din;
         a.hits = dout;
         a.n = cnt;
+        a.counter = next_counter();
         a.node_tests = counted ? dcounts + slot * 2 * kChunkRays : nullptr;
         a.tri_tests = counted ? dcounts + slot * 2 * kChunkRays + cnt : nullptr;
         cudaError_t e = launch_trace(a, st[slot]);
@@ -199,6 +204,95 @@ int scene_trace(pt_scene* s, const pt_ray* rays, uint64_t n, pt_hit* hits, uint3
     int err = 0;
     PT_CUDA(cudaMemcpy(&err, s->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) return fail(PT_ESTACK, "a ray exceeded the traversal stack (malformed or too deep tree)");
+    return PT_OK;
+}
+
+
+// Host-side layout of a scene (everything pt_scene_create uploads).
+int prepare_scene_host(const pt_scene_desc* desc, HostScene& h) {
+    if (!desc->meshes || desc->num_meshes == 0) return fail(PT_EINVAL, "scene has no meshes");
+    for (uint32_t m = 0; m < desc->num_meshes; ++m) {
+        const pt_mesh_desc& d = desc->meshes[m];
+        if (d.material != PT_MAT_LAMBERT && d.material != PT_MAT_MIRROR)
+            return fail(PT_EINVAL, "mesh " + std::to_string(m) + ": unknown material");
+    }
+    WorldMeshes w;
+    int rc = bake_world(desc->meshes, desc->num_meshes, w);
+    if (rc) return rc;
+    BuiltTree t;
+    if (desc->nodes) {
+        if (!desc->leaf_pairs) return fail(PT_EINVAL, "nodes given without leaf_pairs");
+        t.nodes.assign(desc->nodes, desc->nodes + desc->num_nodes);
+        t.leaf_pairs.assign(desc->leaf_pairs, desc->leaf_pairs + 2 * (size_t)w.num_prims);
+        for (size_t i = 0; i < w.num_prims; ++i) {
+            const uint32_t m = t.leaf_pairs[2 * i], f = t.leaf_pairs[2 * i + 1];
+            if (m >= desc->num_meshes || f >= desc->meshes[m].num_faces)
+                return fail(PT_EINVAL, "leaf pair " + std::to_string(i) + " out of range");
+        }
+    } else {
+        rc = build_bvh(desc->meshes, desc->num_meshes, w, 0, t);
+        if (rc) return rc;
+    }
+    rc = validate_tree(t.nodes.data(), (uint32_t)t.nodes.size(), w.num_prims, &h.max_depth);
+    if (rc) return rc;
+    h.num_prims = w.num_prims;
+    h.prim_base = w.prim_base;
+    h.nodes.swap(t.nodes);
+    // faces in leaf order, 48 B each: {v0.xyz v1.x}{v1.yz v2.xy}{v2.z prim mesh 0}
+    h.tris.assign(12 * (size_t)w.num_prims, 0.f);
+    for (size_t i = 0; i < w.num_prims; ++i) {
+        const uint32_t m = t.leaf_pairs[2 * i], f = t.leaf_pairs[2 * i + 1];
+        const uint32_t p = w.prim_base[m] + f;
+        float* o = &h.tris[12 * i];
+        std::memcpy(o, &w.tri[9 * (size_t)p], 9 * sizeof(float));
+        o[9] = bitsf(p);
+        o[10] = bitsf(m);
+    }
+    h.meshes.resize(desc->num_meshes);
+    bool any_normals = false;
+    for (uint32_t m = 0; m < desc->num_meshes; ++m) {
+        const pt_mesh_desc& d = desc->meshes[m];
+        h.meshes[m].material = d.material;
+        h.meshes[m].is_light = d.is_light ? 1 : 0;
+        std::memcpy(h.meshes[m].albedo, d.albedo, sizeof(d.albedo));
+        std::memcpy(h.meshes[m].emission, d.emission, sizeof(d.emission));
+        if (d.nx && d.ny && d.nz) any_normals = true;
+    }
+    if (any_normals) {  // world vertex normals per prim (Transform::ApplyInPlace(Normal&), mesh.cpp:388-400)
+        h.normals.assign(9 * (size_t)w.num_prims, 0.f);
+        for (uint32_t m = 0; m < desc->num_meshes; ++m) {
+            const pt_mesh_desc& d = desc->meshes[m];
+            if (!(d.nx && d.ny && d.nz)) continue;
+            for (uint32_t f = 0; f < d.num_faces; ++f) {
+                const uint32_t vi[3] = {d.fv0[f], d.fv1[f], d.fv2[f]};
+                float* o = &h.normals[9 * (size_t)(w.prim_base[m] + f)];
+                for (int k = 0; k < 3; ++k) {
+                    o[3 * k] = d.nx[vi[k]];
+                    o[3 * k + 1] = d.ny[vi[k]];
+                    o[3 * k + 2] = d.nz[vi[k]];
+                    apply_normal(d.world_to_object, &o[3 * k]);
+                }
+            }
+        }
+    }
+    // area lights (every face of an emitting mesh, mesh/face order): world triangle, then the
+    // running sum of 0.5 * |(v1 - v0) x (v2 - v0)| as the CDF
+    h.light_area = 0.f;
+    for (uint32_t p = 0; p < w.num_prims; ++p) {
+        const uint32_t m = w.prim_mesh[p];
+        if (!desc->meshes[m].is_light) continue;
+        const float* v = &w.tri[9 * (size_t)p];
+        const float e0[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
+        const float e1[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
+        const float c[3] = {e0[1] * e1[2] - e0[2] * e1[1], e0[2] * e1[0] - e0[0] * e1[2], e0[0] * e1[1] - e0[1] * e1[0]};
+        const float area = 0.5f * std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+        h.light_area = h.light_area + area;
+        for (int k = 0; k < 9; ++k) h.light_tris.push_back(v[k]);
+        h.light_tris.push_back(bitsf(p));  // 12 floats per record: v0 v1 v2, prim, mesh, pad
+        h.light_tris.push_back(bitsf(m));
+        h.light_tris.push_back(0.f);
+        h.light_cdf.push_back(h.light_area);
+    }
     return PT_OK;
 }
 
@@ -235,127 +329,39 @@ int pt_bvh_build(const pt_mesh_desc* meshes, uint32_t num_meshes, int threads, p
 int pt_scene_create(const pt_scene_desc* desc, pt_scene** out) {
     if (!desc || !out) return fail(PT_EINVAL, "desc or out is NULL");
     *out = nullptr;
-    if (!desc->meshes || desc->num_meshes == 0) return fail(PT_EINVAL, "scene has no meshes");
     int ndev = 0;
     cudaError_t ce = cudaGetDeviceCount(&ndev);
     if (ce != cudaSuccess || ndev == 0) {
         cudaGetLastError();
         return fail(PT_ECUDA, "no CUDA device available (there is no CPU fallback)");
     }
-    for (uint32_t m = 0; m < desc->num_meshes; ++m) {
-        const pt_mesh_desc& d = desc->meshes[m];
-        if (d.material != PT_MAT_LAMBERT && d.material != PT_MAT_MIRROR)
-            return fail(PT_EINVAL, "mesh " + std::to_string(m) + ": unknown material");
-    }
-    WorldMeshes w;
-    int rc = bake_world(desc->meshes, desc->num_meshes, w);
+    HostScene h;
+    int rc = prepare_scene_host(desc, h);
     if (rc) return rc;
-    BuiltTree t;
-    if (desc->nodes) {
-        if (!desc->leaf_pairs) return fail(PT_EINVAL, "nodes given without leaf_pairs");
-        t.nodes.assign(desc->nodes, desc->nodes + desc->num_nodes);
-        t.leaf_pairs.assign(desc->leaf_pairs, desc->leaf_pairs + 2 * (size_t)w.num_prims);
-        for (size_t i = 0; i < w.num_prims; ++i) {
-            const uint32_t m = t.leaf_pairs[2 * i], f = t.leaf_pairs[2 * i + 1];
-            if (m >= desc->num_meshes || f >= desc->meshes[m].num_faces)
-                return fail(PT_EINVAL, "leaf pair " + std::to_string(i) + " out of range");
-        }
-    } else {
-        rc = build_bvh(desc->meshes, desc->num_meshes, w, 0, t);
-        if (rc) return rc;
-    }
-    uint32_t max_depth = 0;
-    rc = validate_tree(t.nodes.data(), (uint32_t)t.nodes.size(), w.num_prims, &max_depth);
-    if (rc) return rc;
-
     std::unique_ptr<pt_scene> s(new pt_scene());
     cudaGetDevice(&s->device);
-    s->num_nodes = (uint32_t)t.nodes.size();
-    s->num_prims = w.num_prims;
+    s->num_nodes = (uint32_t)h.nodes.size();
+    s->num_prims = h.num_prims;
     s->num_meshes = desc->num_meshes;
-    s->max_depth = max_depth;
-    s->prim_base = w.prim_base;
+    s->max_depth = h.max_depth;
+    s->prim_base = h.prim_base;
     s->has_env = desc->has_env;
     std::memcpy(s->env, desc->env, sizeof(s->env));
-
-    // faces in leaf order, 48 B each: {v0.xyz v1.x}{v1.yz v2.xy}{v2.z prim mesh 0}
-    std::vector<float> tris(12 * (size_t)w.num_prims);
-    for (size_t i = 0; i < w.num_prims; ++i) {
-        const uint32_t m = t.leaf_pairs[2 * i], f = t.leaf_pairs[2 * i + 1];
-        const uint32_t p = w.prim_base[m] + f;
-        const float* v = &w.tri[9 * (size_t)p];
-        float* o = &tris[12 * i];
-        std::memcpy(o, v, 9 * sizeof(float));
-        o[9] = bitsf(p);
-        o[10] = bitsf(m);
-        o[11] = 0.f;
-    }
-    // per-mesh shading records
-    std::vector<DeviceMesh> dm(desc->num_meshes);
-    bool any_normals = false;
-    for (uint32_t m = 0; m < desc->num_meshes; ++m) {
-        const pt_mesh_desc& d = desc->meshes[m];
-        dm[m].material = d.material;
-        dm[m].is_light = d.is_light ? 1 : 0;
-        std::memcpy(dm[m].albedo, d.albedo, sizeof(dm[m].albedo));
-        std::memcpy(dm[m].emission, d.emission, sizeof(dm[m].emission));
-        if (d.nx && d.ny && d.nz) any_normals = true;
-    }
-    s->has_normals = any_normals;
-    std::vector<float> normals;
-    if (any_normals) {  // world vertex normals per prim (Transform::ApplyInPlace(Normal&), mesh.cpp:388-400)
-        normals.assign(9 * (size_t)w.num_prims, 0.f);
-        for (uint32_t m = 0; m < desc->num_meshes; ++m) {
-            const pt_mesh_desc& d = desc->meshes[m];
-            if (!(d.nx && d.ny && d.nz)) continue;
-            for (uint32_t f = 0; f < d.num_faces; ++f) {
-                const uint32_t vi[3] = {d.fv0[f], d.fv1[f], d.fv2[f]};
-                float* o = &normals[9 * (size_t)(w.prim_base[m] + f)];
-                for (int k = 0; k < 3; ++k) {
-                    o[3 * k] = d.nx[vi[k]];
-                    o[3 * k + 1] = d.ny[vi[k]];
-                    o[3 * k + 2] = d.nz[vi[k]];
-                    apply_normal(d.world_to_object, &o[3 * k]);
-                }
-            }
-        }
-    }
-    // area lights (every face of an emitting mesh, mesh/face order): world triangle + CDF of
-    // 0.5 * |(v1 - v0) x (v2 - v0)|
-    std::vector<float> lt, lcdf;
-    float larea = 0.f;
-    for (uint32_t p = 0; p < w.num_prims; ++p) {
-        const uint32_t m = w.prim_mesh[p];
-        if (!desc->meshes[m].is_light) continue;
-        const float* v = &w.tri[9 * (size_t)p];
-        const float e0[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
-        const float e1[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
-        const float c[3] = {e0[1] * e1[2] - e0[2] * e1[1], e0[2] * e1[0] - e0[0] * e1[2], e0[0] * e1[1] - e0[1] * e1[0]};
-        const float area = 0.5f * std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
-        larea = larea + area;
-        for (int k = 0; k < 9; ++k) lt.push_back(v[k]);
-        lt.push_back(bitsf(p));
-        lt.push_back(bitsf(m));
-        lt.push_back(0.f);
-        lt.push_back(0.f);
-        lcdf.push_back(larea);
-    }
-    s->dev.num_lights = (uint32_t)lcdf.size();
-    s->dev.light_area = larea;
+    s->has_normals = !h.normals.empty();
+    s->dev.num_lights = (uint32_t)h.light_cdf.size();
+    s->dev.light_area = h.light_area;
 
     DeviceGuard g(s->device);
     uint64_t bytes = 0;
-    if ((rc = upload(&s->dev.nodes, t.nodes.data(), t.nodes.size(), bytes))) { free_scene(s.release()); return rc; }
-    if ((rc = upload(&s->dev.tris, tris.data(), tris.size(), bytes))) { free_scene(s.release()); return rc; }
-    if ((rc = upload(&s->dev.meshes, dm.data(), dm.size(), bytes))) { free_scene(s.release()); return rc; }
-    if ((rc = upload(&s->dev.prim_tri, w.tri.data(), w.tri.size(), bytes))) { free_scene(s.release()); return rc; }
-    if (any_normals && (rc = upload(&s->dev.prim_normals, normals.data(), normals.size(), bytes))) { free_scene(s.release()); return rc; }
-    if (!lt.empty()) {
-        if ((rc = upload(&s->dev.light_tris, lt.data(), lt.size(), bytes))) { free_scene(s.release()); return rc; }
-        if ((rc = upload(&s->dev.light_cdf, lcdf.data(), lcdf.size(), bytes))) { free_scene(s.release()); return rc; }
-    }
+    if ((rc = upload(&s->dev.nodes, h.nodes.data(), h.nodes.size(), bytes))) { free_scene(s.release()); return rc; }
+    if ((rc = upload(&s->dev.tris, h.tris.data(), h.tris.size(), bytes))) { free_scene(s.release()); return rc; }
+    if ((rc = upload(&s->dev.meshes, h.meshes.data(), h.meshes.size(), bytes))) { free_scene(s.release()); return rc; }
+    if ((rc = upload(&s->dev.prim_normals, h.normals.data(), h.normals.size(), bytes))) { free_scene(s.release()); return rc; }
+    if ((rc = upload(&s->dev.light_tris, h.light_tris.data(), h.light_tris.size(), bytes))) { free_scene(s.release()); return rc; }
+    if ((rc = upload(&s->dev.light_cdf, h.light_cdf.data(), h.light_cdf.size(), bytes))) { free_scene(s.release()); return rc; }
     if (cudaMalloc(&s->err_flag, sizeof(int)) != cudaSuccess) { free_scene(s.release()); return fail(PT_ENOMEM, "cudaMalloc error flag"); }
     cudaMemset(s->err_flag, 0, sizeof(int));
+    if (cudaMalloc(&s->ray_counters, 8 * PT_RAY_COUNTERS) != cudaSuccess) { free_scene(s.release()); return fail(PT_ENOMEM, "cudaMalloc ray counters"); }
     s->device_bytes = bytes;
     *out = s.release();
     return PT_OK;

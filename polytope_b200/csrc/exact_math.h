@@ -43,6 +43,26 @@ PT_HD int clz64(uint64_t x) { return x ? __builtin_clzll(x) : 64; }
 #endif
 PT_HD float fabs_(float a) { return bitsf(fbits(a) & 0x7FFFFFFFu); }
 
+// Read-only loads and the error flag, portable so the path code also builds for the host
+// (used only by an off-line debugging harness; the library never runs it on the CPU).
+template <class T>
+PT_HD T ldg(const T* p) {
+#ifdef __CUDA_ARCH__
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+PT_HD void raise_flag(int* flag) {
+#ifdef __CUDA_ARCH__
+    atomicExch(flag, 1);
+#else
+    *flag = 1;
+#endif
+}
+PT_HD float next_up(float x) { return nextafterf(x, bitsf(0x7F800000u)); }
+PT_HD float next_down(float x) { return nextafterf(x, bitsf(0xFF800000u)); }
+
 // constants.h:62,142-148: gamma_n = (n * eps) / (1 - n * eps) with eps = 2^-24, in float, and
 // BoundingBox.cpp:27: 1 + 2 * Gamma(3).  Bit patterns (checked against the host compiler's
 // constant folding by the CPU tests).
@@ -138,7 +158,12 @@ PT_HD float to_float(uint32_t sign, uint64_t q, int e) {
 }
 }  // namespace detail
 
-PT_HD float f64_diff_emulated(float a, float b, float c, float d) {
+#ifdef __CUDACC__
+inline __host__ __device__ __noinline__  // rare path: kept out of line to spare registers
+#else
+inline
+#endif
+float f64_diff_emulated(float a, float b, float c, float d) {
     using namespace detail;
     const Prod A = product(a, b);
     Prod B = product(c, d);

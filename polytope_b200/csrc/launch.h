@@ -17,6 +17,7 @@ struct TraceArgs {
     uint32_t* node_tests;  // optional
     uint32_t* tri_tests;   // optional
     int* err;              // device flag, set to 1 when a ray overflowed its stack
+    void* counter;         // device 64-bit ray counter for the persistent kernel (null: one thread per ray)
 };
 
 cudaError_t launch_trace(const TraceArgs& a, cudaStream_t s);

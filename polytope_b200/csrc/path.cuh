@@ -1,0 +1,149 @@
+// path.cuh -- one path of the patched PathTraceIntegrator::GetSample
+// (src/cpu/integrators/PathTraceIntegrator.cpp:10-135) as host/device code: the per-hit shading
+// step shared by the fused and the wavefront kernels, the camera ray of a path and the fused path
+// loop.  The kernels in render.cu are the only callers in the library; the functions are also
+// host-compilable so that an off-line harness can run the exact kernel arithmetic on a CPU.
+#pragma once
+
+#include "shade.cuh"
+
+namespace pt {
+
+struct PathState {
+    F3 o, d;
+    F3 src;        // throughput (ReflectanceSpectrum src)
+    F3 L;          // accumulated radiance
+    uint32_t bounces;
+    uint32_t last_lambert;
+};
+
+struct ShadowReq {
+    F3 o, wi;
+    float tmax;
+    F3 contrib;
+    bool valid;
+};
+
+PT_HD bool throughput_is_zero(const F3& s) {  // ReflectanceSpectrum::is_zero
+    return s.x < 0.0039f && s.y < 0.0039f && s.z < 0.0039f;
+}
+
+// One loop iteration of PathTraceIntegrator::GetSample after the intersection (lines 46-132 of
+// PathTraceIntegrator.cpp, patched as described in shade.cuh).  Returns true when the path goes on
+// with the new ray in s.o / s.d; fills `sh` when a shadow ray must be traced.
+PT_HD bool shade_hit(const RenderParams& p, PathState& s, uint32_t prim, uint32_t leaf, float u,
+                                          float v, float w, uint32_t pixel, uint32_t sample, ShadowReq& sh) {
+    sh.valid = false;
+    const bool nee = (p.flags & PT_RENDER_NEE) && p.num_lights > 0;
+    if (prim == kPrimNone) {
+        if (p.has_env) s.L = vadd(s.L, f3(fmul(p.env[0], s.src.x), fmul(p.env[1], s.src.y), fmul(p.env[2], s.src.z)));
+        return false;
+    }
+    F3 v0, v1, v2;
+    uint32_t mesh;
+    load_face((const float4*)p.tris, leaf, v0, v1, v2, mesh);
+    const MeshRec mr = ((const MeshRec*)p.meshes)[mesh];
+    if (mr.is_light) {
+        if (!(nee && s.last_lambert))
+            s.L = vadd(s.L, f3(fmul(mr.emission[0], s.src.x), fmul(mr.emission[1], s.src.y), fmul(mr.emission[2], s.src.z)));
+        return false;
+    }
+    if (s.bounces >= p.max_depth) return false;
+    const uint32_t bounce = s.bounces++;
+    const HitFrame fr = hit_frame(v0, v1, v2, u, v, w, s.d, p.prim_normals ? p.prim_normals + 9 * (size_t)prim : nullptr);
+    uint32_t r[4] = {pixel, sample, bounce, 0u};
+    philox4x32(r, p.seed_lo, p.seed_hi);
+    const F3 d = s.d;
+    const F3 li = vnorm(f3(vdot(d, fr.t1), vdot(d, fr.n), vdot(d, fr.t2)));
+    F3 lo;
+    const bool mirror = mr.material == PT_MAT_MIRROR;
+    if (mirror) {
+        lo = f3(li.x, -li.y, li.z);
+    } else {
+        const float u0 = u01(r[0]), u1 = u01(r[1]);
+        const float rr = fsqrt(u0);
+        float sn, cs;
+        sincos_2pi(u1, sn, cs);
+        const float one_minus = fsub(1.0f, u0);
+        lo = f3(fmul(rr, cs), fsqrt(0.0f < one_minus ? one_minus : 0.0f), fmul(rr, sn));
+        if (nee) {
+            uint32_t r2[4] = {pixel, sample, bounce, 1u};
+            philox4x32(r2, p.seed_lo, p.seed_hi);
+            const LightSample ls = sample_light(p, fr, u01(r[2]), u01(r[3]), u01(r2[0]));
+            if (ls.valid) {
+                sh.valid = true;
+                sh.o = fr.loc;
+                sh.wi = ls.wi;
+                sh.tmax = fmul(ls.dist, 0.999f);
+                sh.contrib = f3(fmul(fmul(fmul(s.src.x, mr.albedo[0]), ls.le.x), ls.wgt),
+                                fmul(fmul(fmul(s.src.y, mr.albedo[1]), ls.le.y), ls.wgt),
+                                fmul(fmul(fmul(s.src.z, mr.albedo[2]), ls.le.z), ls.wgt));
+            }
+        }
+    }
+    s.d = vnorm(f3(fadd(fadd(fmul(fr.t1.x, lo.x), fmul(fr.n.x, lo.y)), fmul(fr.t2.x, lo.z)),
+                   fadd(fadd(fmul(fr.t1.y, lo.x), fmul(fr.n.y, lo.y)), fmul(fr.t2.y, lo.z)),
+                   fadd(fadd(fmul(fr.t1.z, lo.x), fmul(fr.n.z, lo.y)), fmul(fr.t2.z, lo.z))));
+    s.o = fr.loc;
+    s.src = f3(fmul(s.src.x, mr.albedo[0]), fmul(s.src.y, mr.albedo[1]), fmul(s.src.z, mr.albedo[2]));
+    s.last_lambert = mirror ? 0u : 1u;
+    return true;
+}
+
+// Camera ray of a path (pixel centre, or jittered with the (pixel, sample, 0xFFFF) RNG block).
+PT_HD void path_camera(const RenderParams& p, uint64_t path, uint32_t& pixel, uint32_t& sample,
+                                            F3& o, F3& d) {
+    const uint32_t npix = p.width * p.height;
+    sample = (uint32_t)(path / npix);
+    pixel = (uint32_t)(path % npix);
+    const uint32_t x = pixel % p.width, y = pixel / p.width;
+    float px = (float)x + 0.5f, py = (float)y + 0.5f;
+    if (p.flags & PT_RENDER_JITTER) {
+        uint32_t r[4] = {pixel, sample, 0xFFFFu, 0u};
+        philox4x32(r, p.seed_lo, p.seed_hi);
+        px = fadd((float)x, u01(r[0]));
+        py = fadd((float)y, u01(r[1]));
+    }
+    camera_ray(p.cam, px, py, o, d);
+}
+
+PT_HD void clamp_store(float* out, const F3& L) {  // BoxFilter::AddSample clamp
+    out[0] = L.x > 255 ? 255.f : L.x;
+    out[1] = L.y > 255 ? 255.f : L.y;
+    out[2] = L.z > 255 ? 255.f : L.z;
+}
+
+// ---- fused pipeline -------------------------------------------------------------------------
+
+PT_HD void path_fused(const RenderParams& p, uint64_t path, float* out, uint32_t* primary) {
+    const uint4* nodes = (const uint4*)p.nodes;
+    const float4* tris = (const float4*)p.tris;
+    const float inf = bitsf(0x7F800000u);
+    uint32_t pixel, sample;
+    PathState s;
+    path_camera(p, path, pixel, sample, s.o, s.d);
+    s.src = f3(1.f, 1.f, 1.f);
+    s.L = f3(0.f, 0.f, 0.f);
+    s.bounces = 0;
+    s.last_lambert = 0;
+    while (!throughput_is_zero(s.src)) {
+        RayState rs;
+        ray_setup(rs, s.o.x, s.o.y, s.o.z, s.d.x, s.d.y, s.d.z);
+        const TraceResult h = traverse<false>(nodes, tris, p.num_nodes, rs, inf, false);
+        if (h.overflow) { raise_flag(p.err); break; }
+        if (s.bounces == 0 && sample == 0 && primary) primary[pixel] = h.prim;
+        ShadowReq sh;
+        const bool more = shade_hit(p, s, h.prim, h.leaf, h.u, h.v, h.w, pixel, sample, sh);
+        if (sh.valid) {
+            RayState sr;
+            ray_setup(sr, sh.o.x, sh.o.y, sh.o.z, sh.wi.x, sh.wi.y, sh.wi.z);
+            const TraceResult t = traverse<false>(nodes, tris, p.num_nodes, sr, sh.tmax, true);
+            if (t.overflow) { raise_flag(p.err); break; }
+            if (t.prim == kPrimNone) s.L = vadd(s.L, sh.contrib);
+        }
+        if (!more) break;
+    }
+    clamp_store(out, s.L);
+}
+
+}  // namespace pt

@@ -3,12 +3,15 @@
 
 #include <cstdint>
 #include <cstddef>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include "../../include/polytope_b200.h"
 #include "config.h"
+
+#define PT_RAY_COUNTERS 256
 
 namespace pt {
 
@@ -53,6 +56,20 @@ struct DeviceMesh {  // per-mesh shading record (device)
     float emission[3];
 };
 
+struct HostScene {  // host copy of everything a scene handle uploads
+    std::vector<pt_bvh_node> nodes;
+    std::vector<float> tris;          // 12 floats per leaf-ordered face
+    std::vector<DeviceMesh> meshes;
+    std::vector<float> normals;       // 9 floats per prim, empty without vertex normals
+    std::vector<float> light_tris;    // 12 floats per light face
+    std::vector<float> light_cdf;
+    float light_area = 0.f;
+    uint32_t num_prims = 0;
+    uint32_t max_depth = 0;
+    std::vector<uint32_t> prim_base;
+};
+int prepare_scene_host(const pt_scene_desc* desc, HostScene& out);
+
 struct SceneDev {
     // traversal data
     void* nodes = nullptr;        // num_nodes * 32 B  (pt_bvh_node)
@@ -91,4 +108,7 @@ struct pt_scene {
     void* streams[2] = {nullptr, nullptr};
     void* events[4] = {nullptr, nullptr, nullptr, nullptr};
     void* err_flag = nullptr;  // device int, set when a kernel hit a guard
+    // ray counters of the persistent trace kernel: one per launch in flight, taken round-robin
+    void* ray_counters = nullptr;
+    std::atomic<uint32_t> counter_next{0};
 };

@@ -21,23 +21,23 @@ namespace pt {
 
 struct F3 { float x, y, z; };
 
-__device__ __forceinline__ F3 f3(float x, float y, float z) { return {x, y, z}; }
-__device__ __forceinline__ F3 vsub(F3 a, F3 b) { return {fsub(a.x, b.x), fsub(a.y, b.y), fsub(a.z, b.z)}; }
-__device__ __forceinline__ F3 vadd(F3 a, F3 b) { return {fadd(a.x, b.x), fadd(a.y, b.y), fadd(a.z, b.z)}; }
-__device__ __forceinline__ F3 vscale(F3 a, float t) { return {fmul(a.x, t), fmul(a.y, t), fmul(a.z, t)}; }
+PT_HD F3 f3(float x, float y, float z) { return {x, y, z}; }
+PT_HD F3 vsub(F3 a, F3 b) { return {fsub(a.x, b.x), fsub(a.y, b.y), fsub(a.z, b.z)}; }
+PT_HD F3 vadd(F3 a, F3 b) { return {fadd(a.x, b.x), fadd(a.y, b.y), fadd(a.z, b.z)}; }
+PT_HD F3 vscale(F3 a, float t) { return {fmul(a.x, t), fmul(a.y, t), fmul(a.z, t)}; }
 // Vector::Dot: arg.x*self.x + arg.y*self.y + arg.z*self.z (summed left to right)
-__device__ __forceinline__ float vdot(F3 s, F3 a) { return fadd(fadd(fmul(a.x, s.x), fmul(a.y, s.y)), fmul(a.z, s.z)); }
-__device__ __forceinline__ F3 vcross(F3 s, F3 r) {
+PT_HD float vdot(F3 s, F3 a) { return fadd(fadd(fmul(a.x, s.x), fmul(a.y, s.y)), fmul(a.z, s.z)); }
+PT_HD F3 vcross(F3 s, F3 r) {
     return {fsub(fmul(s.y, r.z), fmul(s.z, r.y)), fsub(fmul(s.z, r.x), fmul(s.x, r.z)),
             fsub(fmul(s.x, r.y), fmul(s.y, r.x))};
 }
-__device__ __forceinline__ F3 vnorm(F3 v) {
+PT_HD F3 vnorm(F3 v) {
     const float d = frcp(fsqrt(fadd(fadd(fmul(v.x, v.x), fmul(v.y, v.y)), fmul(v.z, v.z))));
     return {fmul(v.x, d), fmul(v.y, d), fmul(v.z, d)};
 }
 
 // Camera ray through film position (px, py), LeftHanded = true.
-__device__ __forceinline__ void camera_ray(const CameraConst& c, float px, float py, F3& o, F3& d) {
+PT_HD void camera_ray(const CameraConst& c, float px, float py, F3& o, F3& d) {
     const float ndc_x = fmul(px, c.one_over_w);
     const float ndc_y = fmul(py, c.one_over_h);
     const float cx = fmul(fmul(fsub(fmul(2.0f, ndc_x), 1.0f), c.aspect), c.tan_half);
@@ -59,7 +59,7 @@ struct HitFrame {
 };
 
 // Post-hit frame of the committed face (v0, v1, v2 world space).
-__device__ __forceinline__ HitFrame hit_frame(F3 v0, F3 v1, F3 v2, float u, float v, float w, F3 d,
+PT_HD HitFrame hit_frame(F3 v0, F3 v1, F3 v2, float u, float v, float w, F3 d,
                                               const float* __restrict__ vnormals) {
     const float g7 = bitsf(PT_GAMMA7_BITS);
     const F3 err = vscale(f3(fadd(fadd(fabs_(fmul(u, v0.x)), fabs_(fmul(v, v1.x))), fabs_(fmul(w, v2.x))),
@@ -86,10 +86,9 @@ __device__ __forceinline__ HitFrame hit_frame(F3 v0, F3 v1, F3 v2, float u, floa
     F3 off = vscale(n, dd);
     if (vdot(d, n) > 0) off = {-off.x, -off.y, -off.z};
     F3 np = vadd(loc, off);
-    const float inf = __int_as_float(0x7F800000);
-    if (off.x > 0) np.x = nextafterf(np.x, inf); else if (off.x < 0) np.x = nextafterf(np.x, -inf);
-    if (off.y > 0) np.y = nextafterf(np.y, inf); else if (off.y < 0) np.y = nextafterf(np.y, -inf);
-    if (off.z > 0) np.z = nextafterf(np.z, inf); else if (off.z < 0) np.z = nextafterf(np.z, -inf);
+    if (off.x > 0) np.x = next_up(np.x); else if (off.x < 0) np.x = next_down(np.x);
+    if (off.y > 0) np.y = next_up(np.y); else if (off.y < 0) np.y = next_down(np.y);
+    if (off.z > 0) np.z = next_up(np.z); else if (off.z < 0) np.z = next_down(np.z);
     const float d0 = fabs_(vdot(e0, e1)), d1 = fabs_(vdot(e1, e2)), d2 = fabs_(vdot(e2, e0));
     F3 t1;
     if (d0 > d1 && d0 > d2) t1 = e0;
@@ -104,14 +103,14 @@ __device__ __forceinline__ HitFrame hit_frame(F3 v0, F3 v1, F3 v2, float u, floa
     return f;
 }
 
-__device__ __forceinline__ void load_face(const float4* __restrict__ tris, uint32_t leaf, F3& v0, F3& v1, F3& v2,
+PT_HD void load_face(const float4* __restrict__ tris, uint32_t leaf, F3& v0, F3& v1, F3& v2,
                                           uint32_t& mesh) {
-    const float4 q0 = __ldg(tris + 3 * (size_t)leaf), q1 = __ldg(tris + 3 * (size_t)leaf + 1),
-                 q2 = __ldg(tris + 3 * (size_t)leaf + 2);
+    const float4 q0 = ldg(tris + 3 * (size_t)leaf), q1 = ldg(tris + 3 * (size_t)leaf + 1),
+                 q2 = ldg(tris + 3 * (size_t)leaf + 2);
     v0 = f3(q0.x, q0.y, q0.z);
     v1 = f3(q0.w, q1.x, q1.y);
     v2 = f3(q1.z, q1.w, q2.x);
-    mesh = __float_as_uint(q2.z);
+    mesh = fbits(q2.z);
 }
 
 struct MeshRec {
@@ -131,7 +130,7 @@ struct LightSample {
     bool valid;
 };
 
-__device__ __forceinline__ LightSample sample_light(const RenderParams& p, const HitFrame& f, float u_pick, float u_a,
+PT_HD LightSample sample_light(const RenderParams& p, const HitFrame& f, float u_pick, float u_a,
                                                     float u_b) {
     LightSample ls;
     ls.valid = false;
@@ -139,13 +138,13 @@ __device__ __forceinline__ LightSample sample_light(const RenderParams& p, const
     uint32_t lo = 0, hi = p.num_lights - 1;
     while (lo < hi) {
         const uint32_t mid = (lo + hi) / 2;
-        if (target < __ldg(p.light_cdf + mid)) hi = mid; else lo = mid + 1;
+        if (target < ldg(p.light_cdf + mid)) hi = mid; else lo = mid + 1;
     }
     const float* L = p.light_tris + 12 * (size_t)lo;
-    const F3 a = f3(__ldg(L + 0), __ldg(L + 1), __ldg(L + 2));
-    const F3 b = f3(__ldg(L + 3), __ldg(L + 4), __ldg(L + 5));
-    const F3 c = f3(__ldg(L + 6), __ldg(L + 7), __ldg(L + 8));
-    const uint32_t lmesh = __float_as_uint(__ldg(L + 10));
+    const F3 a = f3(ldg(L + 0), ldg(L + 1), ldg(L + 2));
+    const F3 b = f3(ldg(L + 3), ldg(L + 4), ldg(L + 5));
+    const F3 c = f3(ldg(L + 6), ldg(L + 7), ldg(L + 8));
+    const uint32_t lmesh = fbits(ldg(L + 10));
     const float su = fsqrt(u_a);
     const float b0 = fsub(1.0f, su);
     const float b1 = fmul(u_b, su);

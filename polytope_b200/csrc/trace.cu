@@ -38,8 +38,107 @@ __global__ void __launch_bounds__(128) trace_kernel(const uint4* __restrict__ no
     }
 }
 
+// Persistent variant: a grid sized to the SMs; each warp takes chunks of kChunk rays from a global
+// counter and refills a lane as soon as its ray finishes, so lanes stay busy despite rays of very
+// different cost (any-hit rays stop early, closest-hit rays run long).  Each pass of the outer loop
+// runs every active lane's traversal to its next accepted leaf (while-while), then tests that
+// leaf's faces with the other lanes of the warp.  A ray's own node and face order is exactly the
+// reference's; only which rays share a warp changes.
+constexpr uint32_t kChunk = 64;
+
+template <bool COUNT>
+__global__ void __launch_bounds__(128, 8) trace_persistent_kernel(const uint4* __restrict__ nodes,
+                                                               const float4* __restrict__ tris, uint32_t num_nodes,
+                                                               const float4* __restrict__ rays, uint4* __restrict__ hits,
+                                                               uint64_t n, uint32_t* node_tests, uint32_t* tri_tests,
+                                                               int* err, unsigned long long* counter) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    uint64_t pool_next = 0, pool_end = 0;
+    bool exhausted = false, active = false;
+    uint64_t idx = 0;
+    RayWalk k;
+    while (true) {
+        // refill idle lanes from the warp's chunk
+        const uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
+        if (need && !exhausted && pool_next >= pool_end) {
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(counter, (unsigned long long)kChunk);
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (base >= n) {
+                exhausted = true;
+            } else {
+                pool_next = base;
+                pool_end = base + kChunk < n ? base + kChunk : n;
+            }
+        }
+        if (need) {
+            const uint64_t avail = pool_end - pool_next;
+            const uint32_t rank = __popc(need & lt_mask);
+            if (!active && rank < avail) {
+                idx = pool_next + rank;
+                const float4 r0 = __ldg(rays + 2 * idx);
+                const float4 r1 = __ldg(rays + 2 * idx + 1);
+                walk_begin(k, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, r0.w, (__float_as_uint(r1.w) & 1u) != 0);
+                active = true;
+            }
+            const uint64_t took = (uint64_t)__popc(need) < avail ? (uint64_t)__popc(need) : avail;
+            pool_next += took;
+        }
+        if (!__any_sync(0xFFFFFFFFu, active)) {
+            if (exhausted || pool_next >= pool_end) {
+                if (exhausted) break;
+            }
+            continue;
+        }
+        if (active) {
+            uint32_t leaf_off = 0, leaf_n = 0;
+            bool ok = walk_to_leaf<COUNT>(k, nodes, num_nodes, leaf_off, leaf_n);
+            if (ok && leaf_n) walk_leaf<COUNT>(k, tris, leaf_off, leaf_n);
+            if (!ok || k.done || k.sp == 0) {
+                uint4 h;
+                h.x = ok ? k.prim : 0xFFFFFFFEu;
+                h.y = __float_as_uint(k.min_t);
+                h.z = __float_as_uint(k.u);
+                h.w = __float_as_uint(k.v);
+                if (!ok) atomicExch(err, 1);
+                hits[idx] = h;
+                if (COUNT) {
+                    if (node_tests) node_tests[idx] = k.nodes;
+                    if (tri_tests) tri_tests[idx] = k.tris;
+                }
+                active = false;
+            }
+        }
+    }
+}
+
 cudaError_t launch_trace(const TraceArgs& a, cudaStream_t s) {
     if (a.n == 0) return cudaSuccess;
+    if (a.counter) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const bool counted = a.node_tests || a.tri_tests;
+        cudaError_t e = counted ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<true>, 128, 0)
+                                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<false>, 128, 0);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) per_sm = 1;
+        uint64_t grid = (uint64_t)sms * per_sm;
+        const uint64_t need = (a.n + 127) / 128;
+        if (grid > need) grid = need;
+        e = cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s);
+        if (e != cudaSuccess) return e;
+        if (counted)
+            trace_persistent_kernel<true><<<(unsigned)grid, 128, 0, s>>>(
+                (const uint4*)a.nodes, (const float4*)a.tris, a.num_nodes, (const float4*)a.rays, (uint4*)a.hits, a.n,
+                a.node_tests, a.tri_tests, a.err, (unsigned long long*)a.counter);
+        else
+            trace_persistent_kernel<false><<<(unsigned)grid, 128, 0, s>>>(
+                (const uint4*)a.nodes, (const float4*)a.tris, a.num_nodes, (const float4*)a.rays, (uint4*)a.hits, a.n,
+                nullptr, nullptr, a.err, (unsigned long long*)a.counter);
+        return cudaGetLastError();
+    }
     const uint32_t block = 128;
     const uint64_t grid = (a.n + block - 1) / block;
     if (grid > 0x7FFFFFFFull) return cudaErrorInvalidValue;

@@ -37,9 +37,9 @@ struct RayState {
     float dkx, dky, dkz;
 };
 
-__device__ __forceinline__ float sel3(int k, float x, float y, float z) { return k == 0 ? x : (k == 1 ? y : z); }
+PT_HD float sel3(int k, float x, float y, float z) { return k == 0 ? x : (k == 1 ? y : z); }
 
-__device__ __forceinline__ void ray_setup(RayState& r, float ox, float oy, float oz, float dx, float dy, float dz) {
+PT_HD void ray_setup(RayState& r, float ox, float oy, float oz, float dx, float dy, float dz) {
     r.ox = ox; r.oy = oy; r.oz = oz;
     r.dx = dx; r.dy = dy; r.dz = dz;
     r.ix = frcp(dx); r.iy = frcp(dy); r.iz = frcp(dz);
@@ -58,7 +58,7 @@ __device__ __forceinline__ void ray_setup(RayState& r, float ox, float oy, float
 }
 
 // BoundingBox::Hits with the running MinT as the far bound.
-__device__ __forceinline__ bool box_hits(const RayState& r, float b0, float b1, float b2, float b3, float b4, float b5,
+PT_HD bool box_hits(const RayState& r, float b0, float b1, float b2, float b3, float b4, float b5,
                                          float min_t) {
     const bool inside = r.ox > b0 && r.ox < b3 && r.oy > b1 && r.oy < b4 && r.oz > b2 && r.oz < b5;
     if (inside) return true;
@@ -90,7 +90,7 @@ __device__ __forceinline__ bool box_hits(const RayState& r, float b0, float b1, 
     return near_t <= far_t;
 }
 
-__device__ __forceinline__ float max3abs(float x, float y, float z) {  // max_component(abs(v)), mesh.cpp:145-155
+PT_HD float max3abs(float x, float y, float z) {  // max_component(abs(v)), mesh.cpp:145-155
     x = fabs_(x); y = fabs_(y); z = fabs_(z);
     if (x >= y && x >= z) return x;
     if (y >= x && y >= z) return y;
@@ -98,7 +98,7 @@ __device__ __forceinline__ float max3abs(float x, float y, float z) {  // max_co
 }
 
 // One face of Mesh::intersect (mesh.cpp:196-322).  Vertices are world space.
-__device__ __forceinline__ bool wald(const RayState& r, float v0x, float v0y, float v0z, float v1x, float v1y,
+PT_HD bool wald(const RayState& r, float v0x, float v0y, float v0z, float v1x, float v1y,
                                      float v1z, float v2x, float v2y, float v2z, float min_t, float& t_out,
                                      float& u_out, float& v_out, float& w_out) {
     // p_it = permute(v_i - O)
@@ -148,6 +148,80 @@ __device__ __forceinline__ bool wald(const RayState& r, float v0x, float v0y, fl
     return true;
 }
 
+
+// Resumable traversal state of one ray, for kernels that interleave many rays per lane.
+struct RayWalk {
+    RayState r;
+    float min_t;
+    uint32_t prim, leaf;
+    float u, v, w;
+    uint32_t nodes, tris;
+    bool any, done;
+    int sp;
+    uint32_t stack[kStackCap];
+};
+
+PT_HD void walk_begin(RayWalk& k, float ox, float oy, float oz, float dx, float dy, float dz, float tmax, bool any) {
+    ray_setup(k.r, ox, oy, oz, dx, dy, dz);
+    k.min_t = tmax;
+    k.prim = kPrimNone;
+    k.leaf = kPrimNone;
+    k.u = k.v = k.w = 0.f;
+    k.nodes = k.tris = 0;
+    k.any = any;
+    k.done = false;
+    k.sp = 1;
+    k.stack[0] = 0;
+}
+
+// Pops nodes in the reference order until a leaf whose box is hit comes up (returned in
+// leaf_off / leaf_n) or the stack runs empty.  Returns false on a guard failure.
+template <bool COUNT>
+PT_HD bool walk_to_leaf(RayWalk& k, const uint4* __restrict__ nodes, uint32_t num_nodes, uint32_t& leaf_off,
+                        uint32_t& leaf_n) {
+    leaf_n = 0;
+    const bool neg_x = k.r.ix < 0, neg_y = k.r.iy < 0, neg_z = k.r.iz < 0;
+    while (k.sp > 0) {
+        const uint32_t ni = k.stack[--k.sp];
+        if (ni >= num_nodes) return false;
+        const uint4 a = ldg(nodes + 2 * (size_t)ni);
+        const uint4 b = ldg(nodes + 2 * (size_t)ni + 1);
+        if (COUNT) k.nodes++;
+        if (!box_hits(k.r, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), k.min_t)) continue;
+        const uint32_t nf = b.w & 0xFFFFu;
+        if (nf > 0) {
+            leaf_off = b.z;
+            leaf_n = nf;
+            return true;
+        }
+        if (k.sp + 2 > kStackCap) return false;
+        const uint32_t axis = b.w >> 16;
+        const bool neg = axis == 0 ? neg_x : (axis == 1 ? neg_y : neg_z);
+        const uint32_t hi = ni + b.z, lo = ni + 1;
+        k.stack[k.sp++] = neg ? lo : hi;
+        k.stack[k.sp++] = neg ? hi : lo;
+    }
+    return true;
+}
+
+// The faces of one leaf in leaf order (Mesh::intersect per face, bvh.cpp:496-505).
+template <bool COUNT>
+PT_HD void walk_leaf(RayWalk& k, const float4* __restrict__ tris, uint32_t leaf_off, uint32_t leaf_n) {
+    for (uint32_t j = 0; j < leaf_n; ++j) {
+        const size_t ti = 3 * (size_t)(leaf_off + j);
+        const float4 q0 = ldg(tris + ti), q1 = ldg(tris + ti + 1), q2 = ldg(tris + ti + 2);
+        if (COUNT) k.tris++;
+        float t, u, v, w;
+        if (wald(k.r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, k.min_t, t, u, v, w)) {
+            k.min_t = t;
+            k.prim = fbits(q2.y);
+            k.leaf = leaf_off + j;
+            k.u = u; k.v = v; k.w = w;
+            if (k.any) { k.done = true; return; }
+        }
+    }
+}
+
 struct TraceResult {
     uint32_t prim;   // global primitive id or kPrimNone
     uint32_t leaf;   // leaf-ordered index of the committed face
@@ -159,7 +233,7 @@ struct TraceResult {
 // bvh::intersect_compact.  `any` stops at the first accepted face.  COUNT keeps the per-ray node
 // and face test counts (Intersection::num_bb_hits + num_bb_misses, num_triangle_isects).
 template <bool COUNT>
-__device__ __forceinline__ TraceResult traverse(const uint4* __restrict__ nodes, const float4* __restrict__ tris,
+PT_HD TraceResult traverse(const uint4* __restrict__ nodes, const float4* __restrict__ tris,
                                                 uint32_t num_nodes, const RayState& r, float tmax, bool any) {
     TraceResult res;
     res.prim = kPrimNone;
@@ -176,22 +250,22 @@ __device__ __forceinline__ TraceResult traverse(const uint4* __restrict__ nodes,
     while (sp > 0) {
         const uint32_t ni = stack[--sp];
         if (ni >= num_nodes) { res.overflow = true; break; }  // malformed tree guard
-        const uint4 a = __ldg(nodes + 2 * (size_t)ni);
-        const uint4 b = __ldg(nodes + 2 * (size_t)ni + 1);
+        const uint4 a = ldg(nodes + 2 * (size_t)ni);
+        const uint4 b = ldg(nodes + 2 * (size_t)ni + 1);
         if (COUNT) res.nodes++;
-        if (!box_hits(r, __uint_as_float(a.x), __uint_as_float(a.y), __uint_as_float(a.z), __uint_as_float(a.w),
-                      __uint_as_float(b.x), __uint_as_float(b.y), min_t))
+        if (!box_hits(r, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w),
+                      bitsf(b.x), bitsf(b.y), min_t))
             continue;
         const uint32_t nf = b.w & 0xFFFFu;
         if (nf > 0) {
             for (uint32_t k = 0; k < nf; ++k) {
                 const size_t ti = 3 * (size_t)(b.z + k);
-                const float4 q0 = __ldg(tris + ti), q1 = __ldg(tris + ti + 1), q2 = __ldg(tris + ti + 2);
+                const float4 q0 = ldg(tris + ti), q1 = ldg(tris + ti + 1), q2 = ldg(tris + ti + 2);
                 if (COUNT) res.tris++;
                 float t, u, v, w;
                 if (wald(r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, min_t, t, u, v, w)) {
                     min_t = t;
-                    res.prim = __float_as_uint(q2.y);
+                    res.prim = fbits(q2.y);
                     res.leaf = b.z + k;
                     res.t = t; res.u = u; res.v = v; res.w = w;
                     if (any) return res;

@@ -23,24 +23,30 @@ def image_errors(a, b):
     return rel, np.abs(a - b).mean() / max(np.abs(b).mean(), 1e-30)
 
 
-def test_small_scene_render_matches_reference_fixture(cuda_device):
+PIPELINES = [0, pb.RENDER_WAVEFRONT]
+
+
+@pytest.mark.parametrize("pipeline", PIPELINES, ids=["fused", "wavefront"])
+def test_small_scene_render_matches_reference_fixture(cuda_device, pipeline):
     g = load_golden("small_scene.npz")
     meshes, env = W.small_scene()
     scene = pb.Scene(meshes, env)
     for flags, key in ((pb.RENDER_NEE, "nee"), (0, "bsdf")):
-        rgb, prim = pb.render(scene, 80, 60, 4, 4, W.SMALL_CAMERA, seed=1, flags=flags)
+        rgb, prim = pb.render(scene, 80, 60, 4, 4, W.SMALL_CAMERA, seed=1, flags=flags | pipeline)
         rel, mean = image_errors(rgb, g[f"rgb_{key}"])
         assert rel <= REL_RMSE_TOL and mean <= MEAN_ERR_TOL, (key, rel, mean)
         assert_bit_equal(rgb, g[f"rgb_{key}"], f"film {key}")
         assert_bit_equal(prim, g[f"prim_{key}"], f"primary ids {key}")
 
 
-def test_small_scene_full_config_matches_oracle(cuda_device):
+@pytest.mark.parametrize("pipeline", PIPELINES, ids=["fused", "wavefront"])
+def test_small_scene_full_config_matches_oracle(cuda_device, pipeline):
     """320x240, 8 spp, depth 4, NEE: the full small configuration against the CPU oracle."""
     meshes, env = W.small_scene()
     scene = pb.Scene(meshes, env)
     d = W.SMALL_RENDER
-    rgb, prim = pb.render(scene, d["width"], d["height"], d["spp"], d["max_depth"], d["camera"], d["seed"], pb.RENDER_NEE)
+    rgb, prim = pb.render(scene, d["width"], d["height"], d["spp"], d["max_depth"], d["camera"], d["seed"],
+                          pb.RENDER_NEE | pipeline)
     o = po.OracleScene(meshes, env)
     orgb, oprim = o.render(dict(d, flags=1))
     assert_bit_equal(prim, oprim, "primary ids")
@@ -48,16 +54,18 @@ def test_small_scene_full_config_matches_oracle(cuda_device):
     assert rgb.mean() > 1.0
 
 
-def test_instanced_scene_matches_reference_fixture(cuda_device):
+@pytest.mark.parametrize("pipeline", PIPELINES, ids=["fused", "wavefront"])
+def test_instanced_scene_matches_reference_fixture(cuda_device, pipeline):
     g = load_golden("instanced_small.npz")
     im, env = W.instanced_scene(level=4)
     scene = pb.Scene(im, env)
-    rgb, prim = pb.render(scene, 64, 40, 2, 8, W.INSTANCED_CAMERA, seed=1, flags=pb.RENDER_NEE)
+    rgb, prim = pb.render(scene, 64, 40, 2, 8, W.INSTANCED_CAMERA, seed=1, flags=pb.RENDER_NEE | pipeline)
     assert_bit_equal(prim, g["prim"], "primary ids")
     assert_bit_equal(rgb, g["rgb"], "film")
 
 
-@pytest.mark.parametrize("flags", [pb.RENDER_JITTER | pb.RENDER_NEE, pb.RENDER_JITTER])
+@pytest.mark.parametrize("flags", [pb.RENDER_JITTER | pb.RENDER_NEE, pb.RENDER_JITTER,
+                                   pb.RENDER_JITTER | pb.RENDER_NEE | pb.RENDER_WAVEFRONT])
 def test_jitter_and_small_waves(cuda_device, flags):
     meshes, env = W.small_scene(level=3)
     scene = pb.Scene(meshes, env)
