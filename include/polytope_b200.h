@@ -15,7 +15,7 @@
  *   pt_render         <- spawn N x AbstractRunner::Run + join + Output()
  *                        (TileRunner::Run -> AbstractRunner::Trace -> PathTraceIntegrator::GetSample)
  *                                                                   src/cpu/main.cpp:187-220,
- *                                                                   src/cpu/runners/TileRunner.cpp:64-104,
+ *                                                                   src/cpu/runners/TileRunner.cpp:77-117,
  *                                                                   src/cpu/runners/AbstractRunner.cpp:11-31,
  *                                                                   src/cpu/integrators/PathTraceIntegrator.cpp:10-135
  *
