@@ -200,6 +200,24 @@ typedef struct pt_render_desc {
 int pt_render(pt_scene *scene, const pt_render_desc *desc, float *rgb_out,
               uint32_t *primary_prim_out, uint32_t mem_flags, void *stream);
 
+/* Same render as pt_render, for callers that cannot allocate device memory during the call: an
+ * application that owns the whole device-memory budget and forbids allocations after start-up,
+ * or a per-frame loop that cannot afford the device-wide synchronisation of cudaFree.  No
+ * counterpart in the reference.  The scratch (film sums and one wave of path radiance) lives in a
+ * fixed 6 MiB device array inside the library instead of being allocated per call.
+ *   - rgb_dev (width*height*3 floats) and primary_dev (width*height ids, optional) are DEVICE
+ *     pointers owned by the caller; the call is asynchronous on `stream`.
+ *   - At most 262,144 pixels (e.g. 512x512) per frame and 262,144 paths per wave; larger frames
+ *     are rejected with PT_EINVAL.  Only the fused pipeline (no PT_RENDER_WAVEFRONT).
+ *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
+ *     that device current; make that first call before any stream capture.
+ *   - Every call shares the array and it keeps the previous call's contents (the film sums are
+ *     cleared at the start of each call): calls that overlap on the GPU (different streams, or
+ *     different host threads) race and must be serialised by the caller.
+ *   - The call calls no cudaMalloc, cudaFree or allocating library routine. */
+int pt_render_noalloc(pt_scene *scene, const pt_render_desc *desc, float *rgb_dev,
+                      uint32_t *primary_dev, void *stream);
+
 /* ---- synthetic workload generators (deterministic, shared by the checker and the bench) --- */
 
 /* Icosphere: icosahedron subdivided `level` times (20 * 4^level faces, 10 * 4^level + 2

@@ -97,6 +97,7 @@ def _load() -> C.CDLL:
         "pt_trace": (i, [_vp, _vp, u64, _vp, u32, _vp]),
         "pt_trace_counted": (i, [_vp, _vp, u64, _vp, _vp, _vp, u32, _vp]),
         "pt_render": (i, [_vp, C.POINTER(RenderDesc), _vp, _vp, u32, _vp]),
+        "pt_render_noalloc": (i, [_vp, C.POINTER(RenderDesc), _vp, _vp, _vp]),
         "pt_gen_icosphere": (i, [u32, C.c_float, C.c_float, u64, _fp, _fp, _fp, _up, _up, _up, _up, _up]),
         "pt_gen_rays": (i, [u64, C.c_float, u64, _vp]),
         "pt_host_f64_diff_emulated": (C.c_float, [C.c_float] * 4),
