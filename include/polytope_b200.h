@@ -218,6 +218,79 @@ int pt_render(pt_scene *scene, const pt_render_desc *desc, float *rgb_out,
 int pt_render_noalloc(pt_scene *scene, const pt_render_desc *desc, float *rgb_dev,
                       uint32_t *primary_dev, void *stream);
 
+/* ---- batched renders (many uneven scenes in one persistent, graph-captured launch) -------- */
+
+/* One render of a batch.  The batch keeps its own device films; read them with pt_batch_output. */
+typedef struct pt_batch_item {
+    pt_scene      *scene;
+    pt_render_desc desc;              /* fused pipeline only (no PT_RENDER_WAVEFRONT)             */
+} pt_batch_item;
+
+/* Launch shape of the multi-render kernel (chosen by pt_batch_autotune). */
+typedef struct pt_batch_tuning {
+    uint64_t wave_pixels;             /* pixels per launch; 0 = all pixels in one launch          */
+    uint32_t threads_per_block;       /* 64, 128 or 256                                           */
+    uint32_t stack_depth;             /* traversal stack entries (24/32/48/64; 0 = smallest fit)   */
+    uint32_t queue_chunk;             /* pixels a warp takes per fetch (multiple of 32)           */
+} pt_batch_tuning;
+
+typedef struct pt_batch_tune_result {
+    pt_batch_tuning tuning;
+    float           ms;               /* time of one batch replay                                  */
+} pt_batch_tune_result;
+
+typedef struct pt_batch pt_batch;
+
+/* Renders several frames of possibly different scenes, resolutions, spp and depths in persistent
+ * launches that share the GPU pixel by pixel (a lane traces all samples of one pixel, in sample
+ * order, then takes the next pixel of any render).  Every film equals pt_render's bit for bit.
+ * The launch sequence is captured once into a CUDA graph; pt_batch_run replays it.  Replaces
+ * running the reference's render call once per scene (src/cpu/main.cpp:187-220). */
+int pt_batch_default_tuning(pt_batch_tuning *tuning);
+int pt_batch_create(const pt_batch_item *items, uint32_t n, const pt_batch_tuning *tuning, pt_batch **out);
+/* stream == NULL: run on the batch's own stream and wait; otherwise enqueue on `stream`. */
+int pt_batch_run(pt_batch *batch, void *stream);
+/* Host copies of item i's film / primary ids (either may be NULL) and the rays traced (camera,
+ * bounce and shadow rays) by the last run of the whole batch. */
+int pt_batch_output(pt_batch *batch, uint32_t i, float *rgb_out, uint32_t *primary_out, uint64_t *rays_traced);
+int pt_batch_destroy(pt_batch *batch);
+/* Coordinate descent over threads per block, queue chunk, stack depth and wave size, timing each
+ * candidate on the given items (CUDA events, mean of two graph replays after a warm-up).
+ * results (optional) receives up to *num_results timed candidates. */
+int pt_batch_autotune(const pt_batch_item *items, uint32_t n, pt_batch_tuning *best, double *best_ms,
+                      pt_batch_tune_result *results, uint32_t *num_results);
+
+/* ---- serving loop (continuous batching of render requests over resident scenes) ----------- */
+
+typedef struct pt_server_config {
+    uint32_t        max_inflight;     /* requests admitted at once                                 */
+    uint64_t        memory_budget;    /* device bytes for admitted requests' films (0 = 80 % free) */
+    uint64_t        wave_pixels;      /* pixels per wave, shared fairly by admitted requests       */
+    pt_batch_tuning tuning;
+} pt_server_config;
+
+typedef struct pt_server_stats {
+    uint64_t waves, completed, rays_traced;
+    double   busy_ms;                 /* host-measured time the GPU spent on waves                */
+    uint64_t pending, active, device_bytes_in_use;
+} pt_server_stats;
+
+typedef struct pt_server pt_server;
+
+/* A scheduler thread admits queued requests while max_inflight and the memory budget allow and
+ * runs waves that take a fair share of pixels from every admitted request, so requests arriving
+ * while others run join the next wave.  Request states: 0 queued, 1 admitted, 2 done, < 0 error.
+ * A request's film is identical to pt_render's whether it ran alone or in any mix. */
+int pt_server_create(const pt_server_config *cfg, pt_server **out);
+int pt_server_submit(pt_server *server, pt_scene *scene, const pt_render_desc *desc, uint64_t *ticket);
+/* latency_ms: submit to completion (-1 until done). */
+int pt_server_poll(pt_server *server, uint64_t ticket, int *state, double *latency_ms);
+int pt_server_wait(pt_server *server, uint64_t ticket, uint32_t timeout_ms, int *state);
+/* Copies a finished request's film (width*height*3 floats) and primary ids, then forgets it. */
+int pt_server_fetch(pt_server *server, uint64_t ticket, float *rgb_out, uint32_t *primary_out);
+int pt_server_get_stats(pt_server *server, pt_server_stats *stats);
+int pt_server_destroy(pt_server *server);
+
 /* ---- synthetic workload generators (deterministic, shared by the checker and the bench) --- */
 
 /* Icosphere: icosahedron subdivided `level` times (20 * 4^level faces, 10 * 4^level + 2

@@ -81,6 +81,32 @@ class RenderDesc(C.Structure):
                 ("seed", C.c_uint64), ("flags", C.c_uint32), ("wave_paths", C.c_uint32), ("camera", Camera)]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [("scene", _vp), ("desc", RenderDesc)]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("wave_pixels", C.c_uint64), ("threads_per_block", C.c_uint32), ("stack_depth", C.c_uint32),
+                ("queue_chunk", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+class BatchTuneResult(C.Structure):
+    _fields_ = [("tuning", BatchTuning), ("ms", C.c_float)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("max_inflight", C.c_uint32), ("memory_budget", C.c_uint64), ("wave_pixels", C.c_uint64),
+                ("tuning", BatchTuning)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("waves", C.c_uint64), ("completed", C.c_uint64), ("rays_traced", C.c_uint64), ("busy_ms", C.c_double),
+                ("pending", C.c_uint64), ("active", C.c_uint64), ("device_bytes_in_use", C.c_uint64)]
+
+
 def _load() -> C.CDLL:
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"{LIB_PATH} is missing: build it with `make -C polytope_b200/csrc` "
@@ -98,6 +124,20 @@ def _load() -> C.CDLL:
         "pt_trace_counted": (i, [_vp, _vp, u64, _vp, _vp, _vp, u32, _vp]),
         "pt_render": (i, [_vp, C.POINTER(RenderDesc), _vp, _vp, u32, _vp]),
         "pt_render_noalloc": (i, [_vp, C.POINTER(RenderDesc), _vp, _vp, _vp]),
+        "pt_batch_default_tuning": (i, [C.POINTER(BatchTuning)]),
+        "pt_batch_create": (i, [C.POINTER(BatchItem), u32, C.POINTER(BatchTuning), C.POINTER(_vp)]),
+        "pt_batch_run": (i, [_vp, _vp]),
+        "pt_batch_output": (i, [_vp, u32, _vp, _vp, C.POINTER(u64)]),
+        "pt_batch_destroy": (i, [_vp]),
+        "pt_batch_autotune": (i, [C.POINTER(BatchItem), u32, C.POINTER(BatchTuning), C.POINTER(C.c_double),
+                                  C.POINTER(BatchTuneResult), C.POINTER(u32)]),
+        "pt_server_create": (i, [C.POINTER(ServerConfig), C.POINTER(_vp)]),
+        "pt_server_submit": (i, [_vp, _vp, C.POINTER(RenderDesc), C.POINTER(u64)]),
+        "pt_server_poll": (i, [_vp, u64, C.POINTER(i), C.POINTER(C.c_double)]),
+        "pt_server_wait": (i, [_vp, u64, u32, C.POINTER(i)]),
+        "pt_server_fetch": (i, [_vp, u64, _vp, _vp]),
+        "pt_server_get_stats": (i, [_vp, C.POINTER(ServerStats)]),
+        "pt_server_destroy": (i, [_vp]),
         "pt_gen_icosphere": (i, [u32, C.c_float, C.c_float, u64, _fp, _fp, _fp, _up, _up, _up, _up, _up]),
         "pt_gen_rays": (i, [u64, C.c_float, u64, _vp]),
         "pt_host_f64_diff_emulated": (C.c_float, [C.c_float] * 4),
@@ -341,3 +381,126 @@ def selftest_device(which: int, inp: np.ndarray, n: int, seed: int = 0) -> np.nd
     inp = np.ascontiguousarray(inp)
     check(lib.pt_selftest_device(which, inp.ctypes.data, out.ctypes.data, n, seed))
     return out
+
+
+# ---- batched renders -------------------------------------------------------------------------
+
+def default_tuning() -> BatchTuning:
+    t = BatchTuning()
+    check(lib.pt_batch_default_tuning(C.byref(t)))
+    return t
+
+
+def _batch_items(jobs):
+    """jobs: sequence of (Scene, RenderDesc)."""
+    arr = (BatchItem * len(jobs))()
+    for k, (scene, rd) in enumerate(jobs):
+        arr[k].scene = scene.handle
+        arr[k].desc = rd
+    return arr
+
+
+class Batch:
+    """Many renders in one persistent, CUDA-graph-captured launch (pt_batch_*)."""
+
+    def __init__(self, jobs, tuning: Optional[BatchTuning] = None):
+        self.jobs = list(jobs)
+        self._items = _batch_items(self.jobs)
+        h = _vp()
+        check(lib.pt_batch_create(self._items, len(self.jobs), C.byref(tuning) if tuning is not None else None, C.byref(h)))
+        self.handle = h
+
+    def run(self, stream: int = 0):
+        check(lib.pt_batch_run(self.handle, stream or None))
+
+    def output(self, i: int):
+        rd = self.jobs[i][1]
+        rgb = np.zeros((rd.height, rd.width, 3), np.float32)
+        prim = np.zeros((rd.height, rd.width), np.uint32)
+        check(lib.pt_batch_output(self.handle, i, rgb.ctypes.data, prim.ctypes.data, None))
+        return rgb, prim
+
+    def rays_traced(self) -> int:
+        r = C.c_uint64(0)
+        check(lib.pt_batch_output(self.handle, 0, None, None, C.byref(r)))
+        return int(r.value)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib.pt_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune(jobs, max_results: int = 64):
+    """Coordinate-descent search of the batch launch shape; returns (best tuning, best ms, trials)."""
+    items = _batch_items(list(jobs))
+    best = BatchTuning()
+    ms = C.c_double(0)
+    res = (BatchTuneResult * max_results)()
+    n = C.c_uint32(max_results)
+    check(lib.pt_batch_autotune(items, len(jobs), C.byref(best), C.byref(ms), res, C.byref(n)))
+    trials = [(res[k].tuning.as_dict(), float(res[k].ms)) for k in range(n.value)]
+    return best, float(ms.value), trials
+
+
+# ---- serving loop ---------------------------------------------------------------------------
+
+class Server:
+    """Continuous batching of render requests over resident scenes (pt_server_*)."""
+
+    def __init__(self, max_inflight: int = 64, memory_budget: int = 0, wave_pixels: int = 1 << 20,
+                 tuning: Optional[BatchTuning] = None):
+        cfg = ServerConfig()
+        cfg.max_inflight = max_inflight
+        cfg.memory_budget = memory_budget
+        cfg.wave_pixels = wave_pixels
+        cfg.tuning = tuning if tuning is not None else default_tuning()
+        h = _vp()
+        check(lib.pt_server_create(C.byref(cfg), C.byref(h)))
+        self.handle = h
+        self._desc = {}
+
+    def submit(self, scene: Scene, rd: RenderDesc) -> int:
+        t = C.c_uint64(0)
+        check(lib.pt_server_submit(self.handle, scene.handle, C.byref(rd), C.byref(t)))
+        self._desc[t.value] = rd
+        return int(t.value)
+
+    def poll(self, ticket: int):
+        st, lat = C.c_int(0), C.c_double(0)
+        check(lib.pt_server_poll(self.handle, ticket, C.byref(st), C.byref(lat)))
+        return st.value, lat.value
+
+    def wait(self, ticket: int, timeout_ms: int = 60000) -> int:
+        st = C.c_int(0)
+        check(lib.pt_server_wait(self.handle, ticket, timeout_ms, C.byref(st)))
+        return st.value
+
+    def fetch(self, ticket: int):
+        rd = self._desc.pop(ticket)
+        rgb = np.zeros((rd.height, rd.width, 3), np.float32)
+        prim = np.zeros((rd.height, rd.width), np.uint32)
+        check(lib.pt_server_fetch(self.handle, ticket, rgb.ctypes.data, prim.ctypes.data))
+        return rgb, prim
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        check(lib.pt_server_get_stats(self.handle, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib.pt_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

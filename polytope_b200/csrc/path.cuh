@@ -115,7 +115,9 @@ PT_HD void clamp_store(float* out, const F3& L) {  // BoxFilter::AddSample clamp
 
 // ---- fused pipeline -------------------------------------------------------------------------
 
-PT_HD void path_fused(const RenderParams& p, uint64_t path, float* out, uint32_t* primary) {
+// Returns the number of rays traced (camera + bounce + shadow).
+template <int CAP = kStackCap>
+PT_HD uint32_t path_fused(const RenderParams& p, uint64_t path, float* out, uint32_t* primary) {
     const uint4* nodes = (const uint4*)p.nodes;
     const float4* tris = (const float4*)p.tris;
     const float inf = bitsf(0x7F800000u);
@@ -126,10 +128,12 @@ PT_HD void path_fused(const RenderParams& p, uint64_t path, float* out, uint32_t
     s.L = f3(0.f, 0.f, 0.f);
     s.bounces = 0;
     s.last_lambert = 0;
+    uint32_t rays = 0;
     while (!throughput_is_zero(s.src)) {
         RayState rs;
         ray_setup(rs, s.o.x, s.o.y, s.o.z, s.d.x, s.d.y, s.d.z);
-        const TraceResult h = traverse<false>(nodes, tris, p.num_nodes, rs, inf, false);
+        const TraceResult h = traverse<false, CAP>(nodes, tris, p.num_nodes, rs, inf, false);
+        ++rays;
         if (h.overflow) { raise_flag(p.err); break; }
         if (s.bounces == 0 && sample == 0 && primary) primary[pixel] = h.prim;
         ShadowReq sh;
@@ -137,13 +141,15 @@ PT_HD void path_fused(const RenderParams& p, uint64_t path, float* out, uint32_t
         if (sh.valid) {
             RayState sr;
             ray_setup(sr, sh.o.x, sh.o.y, sh.o.z, sh.wi.x, sh.wi.y, sh.wi.z);
-            const TraceResult t = traverse<false>(nodes, tris, p.num_nodes, sr, sh.tmax, true);
+            const TraceResult t = traverse<false, CAP>(nodes, tris, p.num_nodes, sr, sh.tmax, true);
+            ++rays;
             if (t.overflow) { raise_flag(p.err); break; }
             if (t.prim == kPrimNone) s.L = vadd(s.L, sh.contrib);
         }
         if (!more) break;
     }
     clamp_store(out, s.L);
+    return rays;
 }
 
 }  // namespace pt

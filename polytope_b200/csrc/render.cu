@@ -23,8 +23,12 @@ namespace pt {
 __global__ void __launch_bounds__(128) path_kernel(const RenderParams p, uint64_t first, uint32_t count,
                                                    float* __restrict__ radiance, uint32_t* __restrict__ primary) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) return;
-    path_fused(p, first + i, radiance + 3 * (size_t)i, primary);
+    uint32_t rays = 0;
+    if (i < count) rays = path_fused(p, first + i, radiance + 3 * (size_t)i, primary);
+    if (p.rays_traced) {
+        const uint32_t sum = __reduce_add_sync(0xFFFFFFFFu, rays);
+        if ((threadIdx.x & 31u) == 0 && sum) atomicAdd(p.rays_traced, (unsigned long long)sum);
+    }
 }
 
 // ---- wavefront pipeline -----------------------------------------------------------------------

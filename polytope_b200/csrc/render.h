@@ -35,6 +35,7 @@ struct RenderParams {
     uint32_t seed_lo, seed_hi;
     uint32_t flags;
     int* err;
+    unsigned long long* rays_traced;  // optional: counts camera + bounce + shadow rays
 };
 
 // Paths [first, first + count) in sample-major order (path p = sample * W*H + pixel).

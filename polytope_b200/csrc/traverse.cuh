@@ -231,8 +231,9 @@ struct TraceResult {
 };
 
 // bvh::intersect_compact.  `any` stops at the first accepted face.  COUNT keeps the per-ray node
-// and face test counts (Intersection::num_bb_hits + num_bb_misses, num_triangle_isects).
-template <bool COUNT>
+// and face test counts (Intersection::num_bb_hits + num_bb_misses, num_triangle_isects).  CAP is
+// the stack capacity (tree depth + 2 must fit; the host checks before launching).
+template <bool COUNT, int CAP = kStackCap>
 PT_HD TraceResult traverse(const uint4* __restrict__ nodes, const float4* __restrict__ tris,
                                                 uint32_t num_nodes, const RayState& r, float tmax, bool any) {
     TraceResult res;
@@ -243,7 +244,7 @@ PT_HD TraceResult traverse(const uint4* __restrict__ nodes, const float4* __rest
     res.nodes = res.tris = 0;
     res.overflow = false;
     const bool neg_x = r.ix < 0, neg_y = r.iy < 0, neg_z = r.iz < 0;
-    uint32_t stack[kStackCap];
+    uint32_t stack[CAP];
     int sp = 0;
     stack[sp++] = 0;
     float min_t = tmax;
@@ -273,7 +274,7 @@ PT_HD TraceResult traverse(const uint4* __restrict__ nodes, const float4* __rest
             }
             continue;
         }
-        if (sp + 2 > kStackCap) { res.overflow = true; break; }
+        if (sp + 2 > CAP) { res.overflow = true; break; }
         const uint32_t axis = b.w >> 16;
         const bool neg = axis == 0 ? neg_x : (axis == 1 ? neg_y : neg_z);
         const uint32_t hi = ni + b.z, lo = ni + 1;

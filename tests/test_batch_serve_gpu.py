@@ -1,0 +1,112 @@
+"""GPU tests of the batched multi-scene launch (pt_batch_*), its autotuner and the serving loop
+(pt_server_*): every film must equal pt_render's for the same scene and description, bit for bit,
+alone or in any mix."""
+import time
+
+import numpy as np
+import pytest
+
+from conftest import assert_bit_equal
+import polytope_b200 as pb
+from polytope_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def small_jobs(n=10, seed=5):
+    work = W.batched_workload(n, seed=seed, min_tris=500, max_tris=30_000, resolutions=(16, 24, 40), spps=(1, 3, 4))
+    jobs = []
+    for k, (meshes, env, d) in enumerate(work):
+        scene = pb.Scene(meshes, env)
+        flags = pb.RENDER_NEE | (pb.RENDER_JITTER if k % 2 else 0)
+        rd = pb.render_desc(d["width"], d["height"], d["spp"], d["max_depth"], d["camera"], d["seed"], flags)
+        jobs.append((scene, rd))
+    return jobs
+
+
+def solo(scene, rd):
+    return pb.render(scene, rd.width, rd.height, rd.spp, rd.max_depth,
+                     dict(eye=tuple(rd.camera.eye), look_at=tuple(rd.camera.look_at), up=tuple(rd.camera.up),
+                          fov=rd.camera.fov_deg), rd.seed, rd.flags)
+
+
+def test_batch_films_equal_solo_renders(cuda_device):
+    jobs = small_jobs()
+    b = pb.Batch(jobs)
+    b.run()
+    for i, (scene, rd) in enumerate(jobs):
+        rgb, prim = b.output(i)
+        srgb, sprim = solo(scene, rd)
+        assert_bit_equal(rgb, srgb, f"film {i}")
+        assert_bit_equal(prim, sprim, f"prim {i}")
+    assert b.rays_traced() > sum(rd.width * rd.height * rd.spp for _, rd in jobs)
+    b.run()  # graph replay gives the same films
+    assert_bit_equal(b.output(3)[0], solo(*jobs[3])[0], "replay")
+
+
+def test_batch_tunings_and_autotune(cuda_device):
+    jobs = small_jobs(6, seed=9)
+    ref = [solo(s, rd)[0] for s, rd in jobs]
+    for tpb, chunk, stack, wave in ((64, 32, 0, 0), (256, 128, 64, 1000), (128, 64, 48, 3000)):
+        t = pb.BatchTuning(wave, tpb, stack, chunk)
+        b = pb.Batch(jobs, t)
+        b.run()
+        for i in range(len(jobs)):
+            assert_bit_equal(b.output(i)[0], ref[i], f"tuning {tpb}/{chunk}/{stack}/{wave} item {i}")
+    best, ms, trials = pb.autotune(jobs)
+    assert ms > 0 and len(trials) >= 4
+    assert best.threads_per_block in (64, 128, 256) and best.queue_chunk % 32 == 0
+    b = pb.Batch(jobs, best)
+    b.run()
+    assert_bit_equal(b.output(0)[0], ref[0], "autotuned")
+
+
+def test_server_results_same_alone_and_in_the_mix(cuda_device):
+    jobs = small_jobs(12, seed=13)
+    srv = pb.Server(max_inflight=64, wave_pixels=2048)
+    alone = []
+    for scene, rd in jobs:  # one request at a time
+        t = srv.submit(scene, rd)
+        assert srv.wait(t, 60000) == 2
+        alone.append(srv.fetch(t))
+    tickets = [srv.submit(scene, rd) for scene, rd in jobs]  # all at once: interleaved waves
+    for t, (a_rgb, a_prim), (scene, rd) in zip(tickets, alone, jobs):
+        assert srv.wait(t, 60000) == 2
+        st, lat = srv.poll(t)
+        assert st == 2 and lat >= 0
+        rgb, prim = srv.fetch(t)
+        assert_bit_equal(rgb, a_rgb, "mix vs alone")
+        assert_bit_equal(prim, a_prim, "mix vs alone prim")
+        assert_bit_equal(rgb, solo(scene, rd)[0], "server vs pt_render")
+    s = srv.stats()
+    assert s["completed"] == 24 and s["waves"] >= 12 and s["rays_traced"] > 0 and s["device_bytes_in_use"] == 0
+    srv.close()
+
+
+def test_server_admission_by_memory_budget(cuda_device):
+    jobs = small_jobs(6, seed=17)
+    # budget for about one request's film at a time: admissions wait for memory to free up
+    srv = pb.Server(max_inflight=8, memory_budget=40 * 40 * 16 + 4096, wave_pixels=512)
+    tickets = [srv.submit(scene, rd) for scene, rd in jobs]
+    for t, (scene, rd) in zip(tickets, jobs):
+        assert srv.wait(t, 60000) == 2
+        assert_bit_equal(srv.fetch(t)[0], solo(scene, rd)[0], "budgeted")
+    srv.close()
+
+
+def test_server_poisson_arrivals_latency(cuda_device):
+    jobs = small_jobs(8, seed=21)
+    srv = pb.Server(max_inflight=32, wave_pixels=4096)
+    rng = np.random.default_rng(19)
+    tickets = []
+    for i in range(40):
+        time.sleep(float(rng.exponential(1.0 / 500.0)))
+        scene, rd = jobs[int(rng.integers(len(jobs)))]
+        tickets.append(srv.submit(scene, rd))
+    lats = []
+    for t in tickets:
+        assert srv.wait(t, 60000) == 2
+        lats.append(srv.poll(t)[1])
+        srv.fetch(t)
+    assert np.percentile(lats, 99) >= np.percentile(lats, 50) > 0
+    srv.close()
