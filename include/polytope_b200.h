@@ -226,12 +226,20 @@ typedef struct pt_batch_item {
     pt_render_desc desc;              /* fused pipeline only (no PT_RENDER_WAVEFRONT)             */
 } pt_batch_item;
 
-/* Launch shape of the multi-render kernel (chosen by pt_batch_autotune). */
+/* Launch shape of a batch (chosen by pt_batch_autotune).
+ *   PT_PIPELINE_FUSED:     one persistent kernel; a lane traces every sample of a pixel, then
+ *                          takes the next pixel of any render (wave_pixels: pixels per launch).
+ *   PT_PIPELINE_WAVEFRONT: waves of paths of all renders; per bounce a persistent extend kernel,
+ *                          a shade kernel appending to ray / shadow queues, a persistent shadow
+ *                          kernel (wave_pixels: paths per wave). */
+#define PT_PIPELINE_FUSED     0u
+#define PT_PIPELINE_WAVEFRONT 1u
 typedef struct pt_batch_tuning {
-    uint64_t wave_pixels;             /* pixels per launch; 0 = all pixels in one launch          */
+    uint64_t wave_pixels;             /* work per launch / wave; 0 = automatic                    */
     uint32_t threads_per_block;       /* 64, 128 or 256                                           */
     uint32_t stack_depth;             /* traversal stack entries (24/32/48/64; 0 = smallest fit)   */
-    uint32_t queue_chunk;             /* pixels a warp takes per fetch (multiple of 32)           */
+    uint32_t queue_chunk;             /* pixels or rays a warp takes per fetch (multiple of 32)   */
+    uint32_t pipeline;                /* PT_PIPELINE_*                                            */
 } pt_batch_tuning;
 
 typedef struct pt_batch_tune_result {

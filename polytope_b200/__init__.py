@@ -85,9 +85,12 @@ class BatchItem(C.Structure):
     _fields_ = [("scene", _vp), ("desc", RenderDesc)]
 
 
+PIPELINE_FUSED, PIPELINE_WAVEFRONT = 0, 1
+
+
 class BatchTuning(C.Structure):
     _fields_ = [("wave_pixels", C.c_uint64), ("threads_per_block", C.c_uint32), ("stack_depth", C.c_uint32),
-                ("queue_chunk", C.c_uint32)]
+                ("queue_chunk", C.c_uint32), ("pipeline", C.c_uint32)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k, _ in self._fields_}

@@ -19,6 +19,7 @@
 #include "batch.h"
 #include "path.cuh"
 #include "pt_internal.h"
+#include "wavefront.h"
 
 namespace pt {
 
@@ -141,6 +142,7 @@ int check_tuning(const pt_batch_tuning& t) {
     if (t.queue_chunk < 32 || t.queue_chunk > 4096 || (t.queue_chunk & 31u))
         return fail(PT_EINVAL, "queue_chunk must be a multiple of 32 in [32, 4096]");
     if (t.stack_depth > PT_TRAVERSAL_STACK) return fail(PT_EINVAL, "stack_depth above the traversal stack limit");
+    if (t.pipeline != PT_PIPELINE_FUSED && t.pipeline != PT_PIPELINE_WAVEFRONT) return fail(PT_EINVAL, "unknown pipeline");
     return PT_OK;
 }
 
@@ -162,6 +164,16 @@ struct pt_batch {
     void* prims = nullptr;    // all primary ids
     std::vector<size_t> film_off, prim_off;
     void* counters = nullptr; // 2 x u64: ray counter, rays traced
+    void* wf = nullptr;       // wavefront: film sums, items, plan tables, wave state
+    void* wf_films = nullptr;
+    size_t wf_film_bytes = 0;
+    WfPlan plan;
+    WfState ws{};
+    WfTuning wt;
+    WfItem* d_items = nullptr;
+    WfSegment* d_segs = nullptr;
+    WfPixels* d_res = nullptr;
+    WfPixels* d_fin = nullptr;
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -169,10 +181,71 @@ struct pt_batch {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
         if (stream) cudaStreamDestroy(stream);
-        for (void* b : {params, items, films, prims, counters})
+        for (void* b : {params, items, films, prims, counters, wf})
             if (b) cudaFree(b);
     }
 };
+
+namespace {
+// Wavefront pipeline of a batch, before capture: plan the waves over all items' paths, allocate
+// the film sums, the device tables and the wave state in one buffer, and upload the tables.
+int wf_build(pt_batch* b, const pt_batch_item* items, const pt_batch_tuning& t) {
+    std::vector<uint32_t> npix(b->n), spp(b->n), depth(b->n);
+    uint64_t total_paths = 0;
+    for (uint32_t i = 0; i < b->n; ++i) {
+        npix[i] = b->npix[i];
+        spp[i] = items[i].desc.spp;
+        depth[i] = items[i].desc.max_depth;
+        total_paths += (uint64_t)npix[i] * spp[i];
+    }
+    uint64_t wave = t.wave_pixels ? t.wave_pixels : (1ull << 22);
+    if (wave > total_paths) wave = total_paths;
+    if (wave > (1ull << 30)) return fail(PT_EINVAL, "wave above 2^30 paths");
+    wf_plan_all(b->plan, npix, spp, depth, wave);
+    auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    std::vector<size_t> film_off(b->n);
+    size_t film_bytes = 0;
+    for (uint32_t i = 0; i < b->n; ++i) { film_off[i] = film_bytes; film_bytes += up(12 * (size_t)npix[i]); }
+    const WfPlan& plan = b->plan;
+    const size_t item_bytes = up(sizeof(WfItem) * b->n), seg_bytes = up(sizeof(WfSegment) * plan.segments.size());
+    const size_t res_bytes = up(sizeof(WfPixels) * plan.resolve.size());
+    const size_t fin_bytes = up(sizeof(WfPixels) * std::max<size_t>(1, plan.finish.size()));
+    const size_t tables = item_bytes + seg_bytes + res_bytes + fin_bytes;
+    if (cudaMalloc(&b->wf, film_bytes + tables + wf_state_bytes((uint32_t)wave)) != cudaSuccess)
+        return fail(PT_ENOMEM, "cudaMalloc wavefront batch buffers");
+    char* base = (char*)b->wf;
+    b->wf_films = base;
+    b->wf_film_bytes = film_bytes;
+    b->d_items = (WfItem*)(base + film_bytes);
+    b->d_segs = (WfSegment*)(base + film_bytes + item_bytes);
+    b->d_res = (WfPixels*)(base + film_bytes + item_bytes + seg_bytes);
+    b->d_fin = (WfPixels*)(base + film_bytes + item_bytes + seg_bytes + res_bytes);
+    wf_state_carve(base + film_bytes + tables, (uint32_t)wave, b->ws);
+    std::vector<char> host(tables, 0);
+    std::vector<WfItem> hi(b->n);
+    for (uint32_t i = 0; i < b->n; ++i)
+        hi[i] = WfItem{(const RenderParams*)b->params + i, (float*)(base + film_off[i]),
+                       (float*)((char*)b->films + b->film_off[i]), (uint32_t*)((char*)b->prims + b->prim_off[i]), npix[i], spp[i]};
+    std::memcpy(host.data(), hi.data(), sizeof(WfItem) * b->n);
+    std::memcpy(host.data() + item_bytes, plan.segments.data(), sizeof(WfSegment) * plan.segments.size());
+    std::memcpy(host.data() + item_bytes + seg_bytes, plan.resolve.data(), sizeof(WfPixels) * plan.resolve.size());
+    std::memcpy(host.data() + item_bytes + seg_bytes + res_bytes, plan.finish.data(), sizeof(WfPixels) * plan.finish.size());
+    const cudaError_t e = cudaMemcpy(base + film_bytes, host.data(), tables, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return fail(PT_ECUDA, std::string("wavefront tables: ") + cudaGetErrorString(e));
+    b->wt.threads_per_block = t.threads_per_block;
+    b->wt.queue_chunk = t.queue_chunk;
+    b->wt.stack_cap = b->cap;
+    return PT_OK;
+}
+
+// During capture: clear the film sums, then every wave.
+cudaError_t wf_enqueue(pt_batch* b, unsigned long long* rays) {
+    cudaError_t e = cudaMemsetAsync(b->wf_films, 0, b->wf_film_bytes, b->stream);
+    for (size_t k = 0; e == cudaSuccess && k < b->plan.waves.size(); ++k)
+        e = wf_launch_wave(b->d_items, b->d_segs, b->d_res, b->d_fin, b->plan.waves[k], b->ws, b->wt, rays, b->stream);
+    return e;
+}
+}  // namespace
 
 extern "C" int pt_batch_default_tuning(pt_batch_tuning* t) {
     if (!t) return fail(PT_EINVAL, "tuning is NULL");
@@ -180,6 +253,7 @@ extern "C" int pt_batch_default_tuning(pt_batch_tuning* t) {
     t->threads_per_block = 128;
     t->stack_depth = 0;
     t->queue_chunk = 64;
+    t->pipeline = PT_PIPELINE_WAVEFRONT;
     return PT_OK;
 }
 
@@ -240,14 +314,22 @@ extern "C" int pt_batch_create(const pt_batch_item* items, uint32_t n, const pt_
     if (e == cudaSuccess) e = cudaMemcpy(b->items, hi.data(), sizeof(BatchItem) * n, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(PT_ECUDA, std::string("batch setup: ") + cudaGetErrorString(e));
-    // capture: reset the rays-traced counter and the scenes' error flags, then the waves
+    if (t.pipeline == PT_PIPELINE_WAVEFRONT) {
+        rc = wf_build(b.get(), items, t);
+        if (rc) return rc;
+    }
+    // capture: reset the rays-traced counter, then the launches
     unsigned long long* ctr = (unsigned long long*)b->counters;
     e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) e = cudaMemsetAsync(ctr + 1, 0, sizeof(unsigned long long), b->stream);
-    const uint64_t wave = t.wave_pixels ? t.wave_pixels : b->total_pixels;
-    for (uint64_t first = 0; e == cudaSuccess && first < b->total_pixels; first += wave) {
-        const uint64_t cnt = std::min<uint64_t>(wave, b->total_pixels - first);
-        e = launch_batch((const BatchItem*)b->items, n, first, cnt, ctr, t, b->cap, ctr + 1, b->stream);
+    if (t.pipeline == PT_PIPELINE_FUSED) {
+        const uint64_t wave = t.wave_pixels ? t.wave_pixels : b->total_pixels;
+        for (uint64_t first = 0; e == cudaSuccess && first < b->total_pixels; first += wave) {
+            const uint64_t cnt = std::min<uint64_t>(wave, b->total_pixels - first);
+            e = launch_batch((const BatchItem*)b->items, n, first, cnt, ctr, t, b->cap, ctr + 1, b->stream);
+        }
+    } else if (e == cudaSuccess) {
+        e = wf_enqueue(b.get(), ctr + 1);
     }
     cudaGraph_t g = nullptr;
     const cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
@@ -320,11 +402,12 @@ extern "C" int pt_batch_autotune(const pt_batch_item* items, uint32_t n, pt_batc
                                  pt_batch_tune_result* results, uint32_t* num_results) {
     if (!items || !n || !best) return fail(PT_EINVAL, "items or best is NULL");
     uint32_t max_depth = 0;
-    uint64_t total = 0;
+    uint64_t total = 0, total_paths = 0;
     for (uint32_t i = 0; i < n; ++i) {
         if (!items[i].scene) return fail(PT_EINVAL, "NULL scene");
         max_depth = std::max(max_depth, items[i].scene->max_depth);
         total += (uint64_t)items[i].desc.width * items[i].desc.height;
+        total_paths += (uint64_t)items[i].desc.width * items[i].desc.height * items[i].desc.spp;
     }
     const uint32_t cap_results = num_results ? *num_results : 0;
     uint32_t written = 0;
@@ -336,12 +419,24 @@ extern "C" int pt_batch_autotune(const pt_batch_item* items, uint32_t n, pt_batc
     int rc = time_candidate(items, n, cur, cur_ms);
     if (rc) return rc;
     if (results && written < cap_results) results[written++] = pt_batch_tune_result{cur, cur_ms};
-    for (int knob = 0; knob < 4; ++knob) {
+    for (int knob = 0; knob < 5; ++knob) {
         std::vector<pt_batch_tuning> cands;
-        if (knob == 0) for (uint32_t v : {64u, 128u, 256u}) { auto c = cur; c.threads_per_block = v; cands.push_back(c); }
-        if (knob == 1) for (uint32_t v : {32u, 64u, 128u, 256u}) { auto c = cur; c.queue_chunk = v; cands.push_back(c); }
-        if (knob == 2) for (uint32_t v : {24u, 32u, 48u, 64u}) { if (v < max_depth + 2) continue; auto c = cur; c.stack_depth = v; cands.push_back(c); }
-        if (knob == 3) for (uint64_t v : {0ull, 1ull << 20, 1ull << 22}) { if (v && v >= total) continue; auto c = cur; c.wave_pixels = v; cands.push_back(c); }
+        if (knob == 0) for (uint32_t v : {PT_PIPELINE_FUSED, PT_PIPELINE_WAVEFRONT}) { auto c = cur; c.pipeline = v; cands.push_back(c); }
+        if (knob == 1) for (uint32_t v : {64u, 128u, 256u}) { auto c = cur; c.threads_per_block = v; cands.push_back(c); }
+        if (knob == 2) for (uint32_t v : {32u, 64u, 128u, 256u}) { auto c = cur; c.queue_chunk = v; cands.push_back(c); }
+        if (knob == 3) for (uint32_t v : {24u, 32u, 48u, 64u}) { if (v < max_depth + 2) continue; auto c = cur; c.stack_depth = v; cands.push_back(c); }
+        if (knob == 4) {
+            const uint64_t limit = cur.pipeline == PT_PIPELINE_FUSED ? total : total_paths;
+            const uint64_t opts_f[] = {0ull, 1ull << 20, 1ull << 22};
+            const uint64_t opts_w[] = {1ull << 20, 1ull << 22, 1ull << 23};
+            for (int k = 0; k < 3; ++k) {
+                const uint64_t v = cur.pipeline == PT_PIPELINE_FUSED ? opts_f[k] : opts_w[k];
+                if (v && v >= limit) continue;
+                auto c = cur;
+                c.wave_pixels = v;
+                cands.push_back(c);
+            }
+        }
         for (const auto& c : cands) {
             if (std::memcmp(&c, &cur, sizeof(c)) == 0) continue;
             float ms = 0.f;

@@ -46,26 +46,6 @@ cudaError_t launch_resolve_wave(uint64_t first, uint32_t count, uint32_t num_pix
                                 float* film_sum, cudaStream_t s);
 cudaError_t launch_finish_film(const float* film_sum, uint32_t num_pixels, uint32_t spp, float* rgb, cudaStream_t s);
 
-// Per-wave path state and queues of the wavefront pipeline (one slot per path of the wave).
-struct WaveState {
-    float4* ray_o;       // next ray origin
-    float4* ray_d;       // next ray direction
-    float4* thr;         // throughput rgb, w = last bounce was Lambert (bits)
-    float4* rad;         // accumulated radiance rgb
-    uint32_t* bounces;
-    uint4* hit0;         // prim, leaf index, u, v (bits)
-    float* hit1;         // w
-    uint32_t* queue[2];  // extend queues (ping-pong)
-    float4* sh_o;        // shadow rays: origin, tmax
-    float4* sh_d;        // direction, path slot (bits)
-    float4* sh_c;        // contribution rgb if unoccluded
-    uint32_t* counters;  // [0], [1] extend queue lengths, [2] shadow queue length
-};
-size_t wave_state_alloc_bytes(uint32_t count);
-void wave_state_carve(void* base, uint32_t count, WaveState& ws);
-cudaError_t launch_wavefront_wave(const RenderParams& p, uint64_t first, uint32_t count, const WaveState& ws,
-                                  float* radiance, uint32_t* primary, cudaStream_t s);
-
 }  // namespace pt
 
 struct pt_scene;

@@ -150,7 +150,8 @@ PT_HD bool wald(const RayState& r, float v0x, float v0y, float v0z, float v1x, f
 
 
 // Resumable traversal state of one ray, for kernels that interleave many rays per lane.
-struct RayWalk {
+template <int CAP = kStackCap>
+struct RayWalkT {
     RayState r;
     float min_t;
     uint32_t prim, leaf;
@@ -158,10 +159,12 @@ struct RayWalk {
     uint32_t nodes, tris;
     bool any, done;
     int sp;
-    uint32_t stack[kStackCap];
+    uint32_t stack[CAP];
 };
+using RayWalk = RayWalkT<>;
 
-PT_HD void walk_begin(RayWalk& k, float ox, float oy, float oz, float dx, float dy, float dz, float tmax, bool any) {
+template <int CAP>
+PT_HD void walk_begin(RayWalkT<CAP>& k, float ox, float oy, float oz, float dx, float dy, float dz, float tmax, bool any) {
     ray_setup(k.r, ox, oy, oz, dx, dy, dz);
     k.min_t = tmax;
     k.prim = kPrimNone;
@@ -176,8 +179,8 @@ PT_HD void walk_begin(RayWalk& k, float ox, float oy, float oz, float dx, float 
 
 // Pops nodes in the reference order until a leaf whose box is hit comes up (returned in
 // leaf_off / leaf_n) or the stack runs empty.  Returns false on a guard failure.
-template <bool COUNT>
-PT_HD bool walk_to_leaf(RayWalk& k, const uint4* __restrict__ nodes, uint32_t num_nodes, uint32_t& leaf_off,
+template <bool COUNT, int CAP>
+PT_HD bool walk_to_leaf(RayWalkT<CAP>& k, const uint4* __restrict__ nodes, uint32_t num_nodes, uint32_t& leaf_off,
                         uint32_t& leaf_n) {
     leaf_n = 0;
     const bool neg_x = k.r.ix < 0, neg_y = k.r.iy < 0, neg_z = k.r.iz < 0;
@@ -194,7 +197,7 @@ PT_HD bool walk_to_leaf(RayWalk& k, const uint4* __restrict__ nodes, uint32_t nu
             leaf_n = nf;
             return true;
         }
-        if (k.sp + 2 > kStackCap) return false;
+        if (k.sp + 2 > CAP) return false;
         const uint32_t axis = b.w >> 16;
         const bool neg = axis == 0 ? neg_x : (axis == 1 ? neg_y : neg_z);
         const uint32_t hi = ni + b.z, lo = ni + 1;
@@ -205,8 +208,8 @@ PT_HD bool walk_to_leaf(RayWalk& k, const uint4* __restrict__ nodes, uint32_t nu
 }
 
 // The faces of one leaf in leaf order (Mesh::intersect per face, bvh.cpp:496-505).
-template <bool COUNT>
-PT_HD void walk_leaf(RayWalk& k, const float4* __restrict__ tris, uint32_t leaf_off, uint32_t leaf_n) {
+template <bool COUNT, int CAP>
+PT_HD void walk_leaf(RayWalkT<CAP>& k, const float4* __restrict__ tris, uint32_t leaf_off, uint32_t leaf_n) {
     for (uint32_t j = 0; j < leaf_n; ++j) {
         const size_t ti = 3 * (size_t)(leaf_off + j);
         const float4 q0 = ldg(tris + ti), q1 = ldg(tris + ti + 1), q2 = ldg(tris + ti + 2);

@@ -30,9 +30,12 @@ def solo(scene, rd):
                           fov=rd.camera.fov_deg), rd.seed, rd.flags)
 
 
-def test_batch_films_equal_solo_renders(cuda_device):
+@pytest.mark.parametrize("pipeline", [0, 1], ids=["fused", "wavefront"])
+def test_batch_films_equal_solo_renders(cuda_device, pipeline):
     jobs = small_jobs()
-    b = pb.Batch(jobs)
+    t = pb.default_tuning()
+    t.pipeline = pipeline
+    b = pb.Batch(jobs, t)
     b.run()
     for i, (scene, rd) in enumerate(jobs):
         rgb, prim = b.output(i)
@@ -47,8 +50,9 @@ def test_batch_films_equal_solo_renders(cuda_device):
 def test_batch_tunings_and_autotune(cuda_device):
     jobs = small_jobs(6, seed=9)
     ref = [solo(s, rd)[0] for s, rd in jobs]
-    for tpb, chunk, stack, wave in ((64, 32, 0, 0), (256, 128, 64, 1000), (128, 64, 48, 3000)):
-        t = pb.BatchTuning(wave, tpb, stack, chunk)
+    for tpb, chunk, stack, wave, pipe in ((64, 32, 0, 0, 0), (256, 128, 64, 1000, 0), (128, 64, 48, 3000, 0),
+                                          (128, 64, 0, 0, 1), (64, 32, 32, 700, 1), (256, 128, 64, 5000, 1)):
+        t = pb.BatchTuning(wave, tpb, stack, chunk, pipe)
         b = pb.Batch(jobs, t)
         b.run()
         for i in range(len(jobs)):
@@ -61,9 +65,16 @@ def test_batch_tunings_and_autotune(cuda_device):
     assert_bit_equal(b.output(0)[0], ref[0], "autotuned")
 
 
-def test_server_results_same_alone_and_in_the_mix(cuda_device):
+def tuning(pipeline):
+    t = pb.default_tuning()
+    t.pipeline = pipeline
+    return t
+
+
+@pytest.mark.parametrize("pipeline", [0, 1], ids=["fused", "wavefront"])
+def test_server_results_same_alone_and_in_the_mix(cuda_device, pipeline):
     jobs = small_jobs(12, seed=13)
-    srv = pb.Server(max_inflight=64, wave_pixels=2048)
+    srv = pb.Server(max_inflight=64, wave_pixels=2048, tuning=tuning(pipeline))
     alone = []
     for scene, rd in jobs:  # one request at a time
         t = srv.submit(scene, rd)
@@ -83,10 +94,11 @@ def test_server_results_same_alone_and_in_the_mix(cuda_device):
     srv.close()
 
 
-def test_server_admission_by_memory_budget(cuda_device):
+@pytest.mark.parametrize("pipeline", [0, 1], ids=["fused", "wavefront"])
+def test_server_admission_by_memory_budget(cuda_device, pipeline):
     jobs = small_jobs(6, seed=17)
     # budget for about one request's film at a time: admissions wait for memory to free up
-    srv = pb.Server(max_inflight=8, memory_budget=40 * 40 * 16 + 4096, wave_pixels=512)
+    srv = pb.Server(max_inflight=8, memory_budget=40 * 40 * 28 + 4096, wave_pixels=512, tuning=tuning(pipeline))
     tickets = [srv.submit(scene, rd) for scene, rd in jobs]
     for t, (scene, rd) in zip(tickets, jobs):
         assert srv.wait(t, 60000) == 2
