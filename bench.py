@@ -17,6 +17,7 @@ no collective on the data path).
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -97,6 +98,115 @@ def profiled_traffic():
         return None
 
 
+def build_scenes(pb, specs, threads=16):
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(threads) as ex:
+        return list(ex.map(lambda sp: pb.Scene(sp[0], sp[1]), specs))
+
+
+def bench_batched(pb, torch, n_scenes=256):
+    """256 uneven scenes: one autotuned batched launch vs one plain pt_render launch per scene."""
+    import ctypes as C
+    from polytope_b200 import workloads as W
+    work = W.batched_workload(n_scenes)
+    scenes = build_scenes(pb, [(w[0], w[1]) for w in work])
+    jobs = [(sc, pb.render_desc(d["width"], d["height"], d["spp"], d["max_depth"], d["camera"], d["seed"], pb.RENDER_NEE))
+            for sc, (_, _, d) in zip(scenes, work)]
+    outs = [torch.empty(rd.width * rd.height * 3, dtype=torch.float32, device="cuda") for _, rd in jobs]
+
+    def plain():
+        for (sc, rd), o in zip(jobs, outs):
+            pb.check(pb.lib.pt_render(sc.handle, C.byref(rd), o.data_ptr(), None, pb.MEM_DEVICE, None))
+    for (sc, rd), o in zip(jobs[:8], outs):
+        pb.check(pb.lib.pt_render(sc.handle, C.byref(rd), o.data_ptr(), None, pb.MEM_DEVICE, None))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    plain()
+    e1.record()
+    e1.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    best, _, trials = pb.autotune(jobs[::8])
+    b = pb.Batch(jobs, best)
+    b.run()
+    e0.record()
+    b.run()
+    e1.record()
+    e1.synchronize()
+    batch_ms = e0.elapsed_time(e1)
+    rays = b.rays_traced()
+    b.close()
+    return {"workload": f"{n_scenes} scenes (displaced icosphere + boxes, 1k-500k tris log-uniform), 64^2-512^2, 4/16/64 spp, depth 6, NEE",
+            "tris": int(sum(sum(len(m.faces) for m in w[0]) for w in work)),
+            "paths": int(sum(rd.width * rd.height * rd.spp for _, rd in jobs)), "rays": int(rays),
+            "plain_ms": round(plain_ms, 2), "plain_mrays_s": round(rays / plain_ms / 1e3, 1),
+            "batched_ms": round(batch_ms, 2), "batched_mrays_s": round(rays / batch_ms / 1e3, 1),
+            "speedup": round(plain_ms / batch_ms, 3), "tuning": best.as_dict(), "autotune_trials": len(trials),
+            "timing": "CUDA events around 256 sequential pt_render calls (device films) and around one batch graph replay"}
+
+
+def bench_served(pb, torch, n_scenes=32, n_requests=300, rate=200.0, seed=19):
+    """Resident scene pool, Poisson request arrivals: the serving loop vs one pt_render per request
+    in arrival order.  Latency = completion - arrival."""
+    import threading
+    from polytope_b200 import workloads as W
+    pool = W.serving_pool(n_scenes)
+    scenes = build_scenes(pb, pool)
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    reqs = []
+    for k in range(n_requests):
+        res = int(rng.choice([128, 256, 512, 1024]))
+        spp = int(rng.choice([1, 4, 16]))
+        reqs.append((int(rng.integers(n_scenes)), pb.render_desc(res, res, spp, 5, W.SERVE_CAMERA, k + 1, pb.RENDER_NEE)))
+
+    def run_served():
+        srv = pb.Server(max_inflight=64, wave_pixels=1 << 22, tuning=pb.default_tuning())
+        t0 = time.perf_counter()
+        tickets = []
+        for (si, rd), at in zip(reqs, arrivals):
+            now = time.perf_counter() - t0
+            if at > now:
+                time.sleep(at - now)
+            tickets.append(srv.submit(scenes[si], rd))
+        lats = []
+        for t in tickets:
+            srv.wait(t, 600000)
+            lats.append(srv.poll(t)[1])
+            srv.fetch(t)
+        span = time.perf_counter() - t0
+        rays = srv.stats()["rays_traced"]
+        srv.close()
+        return np.array(lats), span, rays
+
+    def run_plain():
+        done = [0.0] * n_requests
+        t0 = time.perf_counter()
+
+        def worker():
+            for k, (si, rd) in enumerate(reqs):
+                now = time.perf_counter() - t0
+                if arrivals[k] > now:
+                    time.sleep(arrivals[k] - now)
+                rgb = np.empty((rd.height, rd.width, 3), np.float32)
+                pb.check(pb.lib.pt_render(scenes[si].handle, ctypes.byref(rd), rgb.ctypes.data, None, 0, None))
+                done[k] = time.perf_counter() - t0
+        th = threading.Thread(target=worker)
+        th.start()
+        th.join()
+        return np.array(done) - arrivals, time.perf_counter() - t0
+
+    lat_s, span_s, rays = run_served()
+    lat_p, span_p = run_plain()
+    lat_p = lat_p * 1000.0
+    pct = lambda a, q: round(float(np.percentile(a, q)), 2)
+    return {"workload": f"{n_scenes} resident scenes (instanced displaced spheres, 100k-4M tris), {n_requests} Poisson requests at {rate:g}/s, 128^2-1024^2, 1/4/16 spp, depth 5",
+            "rays": int(rays),
+            "served": {"mrays_s": round(rays / span_s / 1e6, 1), "p50_ms": pct(lat_s, 50), "p95_ms": pct(lat_s, 95), "p99_ms": pct(lat_s, 99), "makespan_s": round(span_s, 3)},
+            "plain_per_request": {"mrays_s": round(rays / span_p / 1e6, 1), "p50_ms": pct(lat_p, 50), "p95_ms": pct(lat_p, 95), "p99_ms": pct(lat_p, 99), "makespan_s": round(span_p, 3)},
+            "timing": "host steady clock from first arrival to last completion; per-request latency = completion - arrival"}
+
+
 def make_workload(n_rays):
     from polytope_b200 import workloads as W
     return W.microbench(n_rays=n_rays)
@@ -150,6 +260,9 @@ def main():
     ap.add_argument("--rays", type=int, default=N_RAYS)
     ap.add_argument("--ref-sample", type=int, default=N_RAYS)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -184,6 +297,10 @@ def main():
 
     def step():
         pb.check(pb.lib.pt_trace(scene.handle, d_rays.data_ptr(), n, d_hits.data_ptr(), pb.MEM_DEVICE, stream.cuda_stream))
+
+    if not args.no_autotune:  # launch shape of the ray-query kernel, picked before the timed region
+        scene.autotune_trace(d_rays, d_hits, n)
+    trace_tuning = scene.trace_tuning()
 
     with torch.cuda.stream(stream):
         for _ in range(max(3, args.warmup)):
@@ -243,7 +360,7 @@ def main():
             "config": {"workload": WORKLOAD, "rays_per_gpu": n, "faces": int(sum(len(m.faces) for m in meshes)),
                        "launch": "plain per-frame launch (one trace kernel over all rays)",
                        "l2": "inputs larger than L2 (rays 512 MiB + hits 256 MiB per step); BVH + faces (113 MB) stay L2-resident",
-                       "parallelism": f"replicas x{world}"},
+                       "parallelism": f"replicas x{world}", "trace_tuning": trace_tuning},
             "gpu_launches": args.steps,
             "e2e": {"value": round(e2e, 3), "unit": "Mrays/s", "h2d_bytes_per_step": 32 * n, "d2h_bytes_per_step": 16 * n,
                     "ms_per_step": round(e2e_ms, 4)},
@@ -253,6 +370,10 @@ def main():
             "clocks": clk,
             "step_ms": {"min": round(min(per), 4), "median": round(statistics.median(per), 4), "max": round(max(per), 4)},
         }
+        if not args.no_batched and world == 1:
+            line["batched"] = bench_batched(pb, torch)
+        if not args.no_served and world == 1:
+            line["served"] = bench_served(pb, torch)
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             v, kind, dt = cpu_reference(meshes, rays, args.ref_sample, threads)

@@ -81,6 +81,13 @@ class RenderDesc(C.Structure):
                 ("seed", C.c_uint64), ("flags", C.c_uint32), ("wave_paths", C.c_uint32), ("camera", Camera)]
 
 
+class TraceTuning(C.Structure):
+    _fields_ = [("shared_stack", C.c_uint32), ("queue_chunk", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
 class BatchItem(C.Structure):
     _fields_ = [("scene", _vp), ("desc", RenderDesc)]
 
@@ -126,6 +133,9 @@ def _load() -> C.CDLL:
         "pt_trace": (i, [_vp, _vp, u64, _vp, u32, _vp]),
         "pt_trace_counted": (i, [_vp, _vp, u64, _vp, _vp, _vp, u32, _vp]),
         "pt_render": (i, [_vp, C.POINTER(RenderDesc), _vp, _vp, u32, _vp]),
+        "pt_scene_set_trace_tuning": (i, [_vp, C.POINTER(TraceTuning)]),
+        "pt_scene_get_trace_tuning": (i, [_vp, C.POINTER(TraceTuning)]),
+        "pt_trace_autotune": (i, [_vp, _vp, u64, _vp, C.POINTER(TraceTuning), C.POINTER(C.c_float)]),
         "pt_render_noalloc": (i, [_vp, C.POINTER(RenderDesc), _vp, _vp, _vp]),
         "pt_batch_default_tuning": (i, [C.POINTER(BatchTuning)]),
         "pt_batch_create": (i, [C.POINTER(BatchItem), u32, C.POINTER(BatchTuning), C.POINTER(_vp)]),
@@ -306,6 +316,20 @@ class Scene:
             return hits, nt, tt
         check(lib.pt_trace(self.handle, _ptr(rays), n, _ptr(hits), flags, stream or None))
         return hits
+
+    def set_trace_tuning(self, shared_stack: int, queue_chunk: int):
+        check(lib.pt_scene_set_trace_tuning(self.handle, C.byref(TraceTuning(shared_stack, queue_chunk))))
+
+    def trace_tuning(self) -> dict:
+        t = TraceTuning()
+        check(lib.pt_scene_get_trace_tuning(self.handle, C.byref(t)))
+        return t.as_dict()
+
+    def autotune_trace(self, d_rays, d_hits, n: int):
+        """Times the ray-query launch shapes on device buffers; keeps and returns the fastest."""
+        t, ms = TraceTuning(), C.c_float(0)
+        check(lib.pt_trace_autotune(self.handle, _ptr(d_rays), n, _ptr(d_hits), C.byref(t), C.byref(ms)))
+        return t.as_dict(), float(ms.value)
 
     def prim_to_mesh_face(self, prim: np.ndarray):
         prim = np.asarray(prim, np.int64)

@@ -117,6 +117,8 @@ int scene_trace(pt_scene* s, const pt_ray* rays, uint64_t n, pt_hit* hits, uint3
     a.tris = s->dev.tris;
     a.num_nodes = s->num_nodes;
     a.err = (int*)s->err_flag;
+    a.shared_stack = (int)s->trace_tuning.shared_stack;
+    a.chunk = s->trace_tuning.queue_chunk;
     auto next_counter = [s]() {
         return (void*)((unsigned long long*)s->ray_counters + (s->counter_next.fetch_add(1) % PT_RAY_COUNTERS));
     };
@@ -391,6 +393,69 @@ int pt_trace_counted(pt_scene* scene, const pt_ray* rays, uint64_t n, pt_hit* hi
                      uint32_t* tri_tests, uint32_t mem_flags, void* stream) {
     if (!node_tests && !tri_tests) return fail(PT_EINVAL, "no count outputs");
     return scene_trace(scene, rays, n, hits, node_tests, tri_tests, mem_flags, stream);
+}
+
+int pt_scene_set_trace_tuning(pt_scene* scene, const pt_trace_tuning* t) {
+    if (!scene || !t) return fail(PT_EINVAL, "scene or tuning is NULL");
+    if (t->shared_stack != 0 && t->shared_stack != 8 && t->shared_stack != 16)
+        return fail(PT_EINVAL, "shared_stack must be 0, 8 or 16");
+    if (t->queue_chunk < 32 || t->queue_chunk > 4096 || (t->queue_chunk & 31u))
+        return fail(PT_EINVAL, "queue_chunk must be a multiple of 32 in [32, 4096]");
+    scene->trace_tuning = *t;
+    return PT_OK;
+}
+
+int pt_scene_get_trace_tuning(const pt_scene* scene, pt_trace_tuning* t) {
+    if (!scene || !t) return fail(PT_EINVAL, "scene or tuning is NULL");
+    *t = scene->trace_tuning;
+    return PT_OK;
+}
+
+int pt_trace_autotune(pt_scene* scene, const pt_ray* rays_dev, uint64_t n, pt_hit* hits_dev, pt_trace_tuning* best,
+                      float* best_ms) {
+    if (!scene || !rays_dev || !hits_dev || !n) return fail(PT_EINVAL, "scene, rays or hits is NULL");
+    const pt_trace_tuning saved = scene->trace_tuning;
+    pt_trace_tuning cur = saved;
+    float cur_ms = 1e30f;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto time_it = [&](const pt_trace_tuning& t, float& ms) -> int {
+        scene->trace_tuning = t;
+        int rc = pt_trace(scene, rays_dev, n, hits_dev, PT_MEM_DEVICE, nullptr);  // warm-up
+        if (rc) return rc;
+        cudaEventRecord(e0, 0);
+        for (int r = 0; r < 3; ++r)
+            if ((rc = pt_trace(scene, rays_dev, n, hits_dev, PT_MEM_DEVICE, nullptr))) return rc;
+        cudaEventRecord(e1, 0);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&ms, e0, e1);
+        ms /= 3.f;
+        return PT_OK;
+    };
+    int rc = PT_OK;
+    for (uint32_t sh : {0u, 8u, 16u}) {
+        pt_trace_tuning t = cur;
+        t.shared_stack = sh;
+        float ms = 0.f;
+        if ((rc = time_it(t, ms))) break;
+        if (ms < cur_ms) { cur_ms = ms; cur = t; }
+    }
+    for (uint32_t ch : {32u, 64u, 128u, 256u}) {
+        if (rc) break;
+        pt_trace_tuning t = cur;
+        t.queue_chunk = ch;
+        float ms = 0.f;
+        if ((rc = time_it(t, ms))) break;
+        if (ms < cur_ms) { cur_ms = ms; cur = t; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    scene->trace_tuning = rc ? saved : cur;
+    if (rc) return rc;
+    if (best) *best = cur;
+    if (best_ms) *best_ms = cur_ms;
+    return PT_OK;
 }
 
 // ---- exact-arithmetic hooks for the parity tests ------------------------------------------------

@@ -18,6 +18,8 @@ struct TraceArgs {
     uint32_t* tri_tests;   // optional
     int* err;              // device flag, set to 1 when a ray overflowed its stack
     void* counter;         // device 64-bit ray counter for the persistent kernel (null: one thread per ray)
+    int shared_stack;      // stack entries per lane kept in shared memory (0, 8 or 16)
+    uint32_t chunk;        // rays a warp takes per fetch (0 = 64)
 };
 
 cudaError_t launch_trace(const TraceArgs& a, cudaStream_t s);

@@ -111,4 +111,5 @@ struct pt_scene {
     // ray counters of the persistent trace kernel: one per launch in flight, taken round-robin
     void* ray_counters = nullptr;
     std::atomic<uint32_t> counter_next{0};
+    pt_trace_tuning trace_tuning{16, 64};
 };

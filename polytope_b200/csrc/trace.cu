@@ -44,20 +44,21 @@ __global__ void __launch_bounds__(128) trace_kernel(const uint4* __restrict__ no
 // runs every active lane's traversal to its next accepted leaf (while-while), then tests that
 // leaf's faces with the other lanes of the warp.  A ray's own node and face order is exactly the
 // reference's; only which rays share a warp changes.
-constexpr uint32_t kChunk = 64;
-
-template <bool COUNT>
+template <bool COUNT, int SH>
 __global__ void __launch_bounds__(128, 8) trace_persistent_kernel(const uint4* __restrict__ nodes,
                                                                const float4* __restrict__ tris, uint32_t num_nodes,
                                                                const float4* __restrict__ rays, uint4* __restrict__ hits,
                                                                uint64_t n, uint32_t* node_tests, uint32_t* tri_tests,
-                                                               int* err, unsigned long long* counter) {
+                                                               int* err, unsigned long long* counter, uint32_t kChunk) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     uint64_t pool_next = 0, pool_end = 0;
     bool exhausted = false, active = false;
     uint64_t idx = 0;
-    RayWalk k;
+    __shared__ uint32_t sstack[SH > 0 ? SH * 128 : 1];
+    RayWalkT<kStackCap, SH> k;
+    k.stack.base = sstack + threadIdx.x;
+    k.stack.stride = 128;
     while (true) {
         // refill idle lanes from the warp's chunk
         const uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
@@ -120,23 +121,26 @@ cudaError_t launch_trace(const TraceArgs& a, cudaStream_t s) {
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const bool counted = a.node_tests || a.tri_tests;
-        cudaError_t e = counted ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<true>, 128, 0)
-                                : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_persistent_kernel<false>, 128, 0);
+        const int sh = a.shared_stack;
+        auto kern_f = sh >= 16 ? trace_persistent_kernel<false, 16> : (sh >= 8 ? trace_persistent_kernel<false, 8> : trace_persistent_kernel<false, 0>);
+        auto kern_t = sh >= 16 ? trace_persistent_kernel<true, 16> : (sh >= 8 ? trace_persistent_kernel<true, 8> : trace_persistent_kernel<true, 0>);
+        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, counted ? kern_t : kern_f, 128, 0);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) per_sm = 1;
         uint64_t grid = (uint64_t)sms * per_sm;
-        const uint64_t need = (a.n + 127) / 128;
+        const uint32_t ch = a.chunk ? a.chunk : 64u;
+        const uint64_t need = ((a.n + ch - 1) / ch * 32 + 127) / 128;
         if (grid > need) grid = need;
         e = cudaMemsetAsync(a.counter, 0, sizeof(unsigned long long), s);
         if (e != cudaSuccess) return e;
         if (counted)
-            trace_persistent_kernel<true><<<(unsigned)grid, 128, 0, s>>>(
-                (const uint4*)a.nodes, (const float4*)a.tris, a.num_nodes, (const float4*)a.rays, (uint4*)a.hits, a.n,
-                a.node_tests, a.tri_tests, a.err, (unsigned long long*)a.counter);
+            kern_t<<<(unsigned)grid, 128, 0, s>>>((const uint4*)a.nodes, (const float4*)a.tris, a.num_nodes,
+                                                  (const float4*)a.rays, (uint4*)a.hits, a.n, a.node_tests, a.tri_tests,
+                                                  a.err, (unsigned long long*)a.counter, a.chunk ? a.chunk : 64u);
         else
-            trace_persistent_kernel<false><<<(unsigned)grid, 128, 0, s>>>(
-                (const uint4*)a.nodes, (const float4*)a.tris, a.num_nodes, (const float4*)a.rays, (uint4*)a.hits, a.n,
-                nullptr, nullptr, a.err, (unsigned long long*)a.counter);
+            kern_f<<<(unsigned)grid, 128, 0, s>>>((const uint4*)a.nodes, (const float4*)a.tris, a.num_nodes,
+                                                  (const float4*)a.rays, (uint4*)a.hits, a.n, nullptr, nullptr, a.err,
+                                                  (unsigned long long*)a.counter, a.chunk ? a.chunk : 64u);
         return cudaGetLastError();
     }
     const uint32_t block = 128;

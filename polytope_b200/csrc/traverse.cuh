@@ -149,8 +149,30 @@ PT_HD bool wald(const RayState& r, float v0x, float v0y, float v0z, float v1x, f
 }
 
 
+// Traversal stack of one lane: the first SH entries live in shared memory (entry k of the lane at
+// base[k * stride], so the lanes of a warp hit consecutive banks), the rest in local memory.
+// SH = 0 keeps the whole stack in local memory (and is the only form the host build uses).
+template <int CAP, int SH>
+struct WalkStack {
+    uint32_t* base;     // this lane's first shared entry (SH > 0)
+    uint32_t stride;    // threads per block
+    uint32_t spill[CAP - SH];
+    PT_HD void put(int i, uint32_t v) {
+        if constexpr (SH > 0) {
+            if (i < SH) { base[i * stride] = v; return; }
+        }
+        spill[i - SH] = v;
+    }
+    PT_HD uint32_t get(int i) const {
+        if constexpr (SH > 0) {
+            if (i < SH) return base[i * stride];
+        }
+        return spill[i - SH];
+    }
+};
+
 // Resumable traversal state of one ray, for kernels that interleave many rays per lane.
-template <int CAP = kStackCap>
+template <int CAP = kStackCap, int SH = 0>
 struct RayWalkT {
     RayState r;
     float min_t;
@@ -159,12 +181,12 @@ struct RayWalkT {
     uint32_t nodes, tris;
     bool any, done;
     int sp;
-    uint32_t stack[CAP];
+    WalkStack<CAP, SH> stack;
 };
 using RayWalk = RayWalkT<>;
 
-template <int CAP>
-PT_HD void walk_begin(RayWalkT<CAP>& k, float ox, float oy, float oz, float dx, float dy, float dz, float tmax, bool any) {
+template <int CAP, int SH>
+PT_HD void walk_begin(RayWalkT<CAP, SH>& k, float ox, float oy, float oz, float dx, float dy, float dz, float tmax, bool any) {
     ray_setup(k.r, ox, oy, oz, dx, dy, dz);
     k.min_t = tmax;
     k.prim = kPrimNone;
@@ -174,18 +196,18 @@ PT_HD void walk_begin(RayWalkT<CAP>& k, float ox, float oy, float oz, float dx, 
     k.any = any;
     k.done = false;
     k.sp = 1;
-    k.stack[0] = 0;
+    k.stack.put(0, 0u);
 }
 
 // Pops nodes in the reference order until a leaf whose box is hit comes up (returned in
 // leaf_off / leaf_n) or the stack runs empty.  Returns false on a guard failure.
-template <bool COUNT, int CAP>
-PT_HD bool walk_to_leaf(RayWalkT<CAP>& k, const uint4* __restrict__ nodes, uint32_t num_nodes, uint32_t& leaf_off,
+template <bool COUNT, int CAP, int SH>
+PT_HD bool walk_to_leaf(RayWalkT<CAP, SH>& k, const uint4* __restrict__ nodes, uint32_t num_nodes, uint32_t& leaf_off,
                         uint32_t& leaf_n) {
     leaf_n = 0;
     const bool neg_x = k.r.ix < 0, neg_y = k.r.iy < 0, neg_z = k.r.iz < 0;
     while (k.sp > 0) {
-        const uint32_t ni = k.stack[--k.sp];
+        const uint32_t ni = k.stack.get(--k.sp);
         if (ni >= num_nodes) return false;
         const uint4 a = ldg(nodes + 2 * (size_t)ni);
         const uint4 b = ldg(nodes + 2 * (size_t)ni + 1);
@@ -201,15 +223,15 @@ PT_HD bool walk_to_leaf(RayWalkT<CAP>& k, const uint4* __restrict__ nodes, uint3
         const uint32_t axis = b.w >> 16;
         const bool neg = axis == 0 ? neg_x : (axis == 1 ? neg_y : neg_z);
         const uint32_t hi = ni + b.z, lo = ni + 1;
-        k.stack[k.sp++] = neg ? lo : hi;
-        k.stack[k.sp++] = neg ? hi : lo;
+        k.stack.put(k.sp++, neg ? lo : hi);
+        k.stack.put(k.sp++, neg ? hi : lo);
     }
     return true;
 }
 
 // The faces of one leaf in leaf order (Mesh::intersect per face, bvh.cpp:496-505).
-template <bool COUNT, int CAP>
-PT_HD void walk_leaf(RayWalkT<CAP>& k, const float4* __restrict__ tris, uint32_t leaf_off, uint32_t leaf_n) {
+template <bool COUNT, int CAP, int SH>
+PT_HD void walk_leaf(RayWalkT<CAP, SH>& k, const float4* __restrict__ tris, uint32_t leaf_off, uint32_t leaf_n) {
     for (uint32_t j = 0; j < leaf_n; ++j) {
         const size_t ti = 3 * (size_t)(leaf_off + j);
         const float4 q0 = ldg(tris + ti), q1 = ldg(tris + ti + 1), q2 = ldg(tris + ti + 2);

@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256) wf_trace_kernel(const WfItem* __restrict_
     const uint4* nodes = nullptr;
     const float4* tris = nullptr;
     int* err = nullptr;
-    RayWalkT<CAP> k;
+    RayWalkT<CAP, 0> k;
     while (true) {
         const uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
         if (need && !exhausted && pool_next >= pool_end) {
