@@ -92,7 +92,7 @@ def peaks():
 def profiled_traffic():
     """DRAM bytes per launch of the trace kernel from the committed ncu summary, if any."""
     try:
-        with open(os.path.join(ROOT, "profiles", "trace_kernel_microbench.json")) as f:
+        with open(os.path.join(ROOT, "profiles", "trace_persistent_kernel_microbench.json")) as f:
             return json.load(f).get("dram_bytes_per_launch_full_size")
     except (OSError, ValueError):
         return None
