@@ -145,66 +145,157 @@ def bench_batched(pb, torch, n_scenes=256):
             "timing": "CUDA events around 256 sequential pt_render calls (device films) and around one batch graph replay"}
 
 
-def bench_served(pb, torch, n_scenes=32, n_requests=300, rate=200.0, seed=19):
-    """Resident scene pool, Poisson request arrivals: the serving loop vs one pt_render per request
-    in arrival order.  Latency = completion - arrival."""
-    import threading
+def bench_render(pb, torch, cpu=True, cpu_rows=16, threads=None):
+    """Full path trace of the instanced scene (6,553,602 tris, 1920x1080, 64 spp, depth 8, NEE):
+    the plain pt_render launch vs the autotuned wave engine on the same frame (a one-item batch),
+    and the film against the reference's CPU render of a band of rows at equal spp."""
+    import ctypes as C
     from polytope_b200 import workloads as W
-    pool = W.serving_pool(n_scenes)
-    scenes = build_scenes(pb, pool)
+    meshes, env = W.instanced_scene()
+    d = dict(W.INSTANCED_RENDER)
+    scene = pb.Scene(meshes, env)
+    rd = pb.render_desc(d["width"], d["height"], d["spp"], d["max_depth"], d["camera"], d["seed"], pb.RENDER_NEE)
+    npix = rd.width * rd.height
+    samples = npix * rd.spp
+    out = torch.empty(npix * 3, dtype=torch.float32, device="cuda")
+    prim = torch.empty(npix, dtype=torch.int32, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(reps):
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    plain_ms = timed(lambda: pb.check(pb.lib.pt_render(scene.handle, C.byref(rd), out.data_ptr(), prim.data_ptr(),
+                                                       pb.MEM_DEVICE, None)))
+    film = out.view(rd.height, rd.width, 3).cpu().numpy()
+    prim_ids = prim.view(rd.height, rd.width).cpu().numpy().view(np.uint32)
+    best, _, trials = pb.autotune([(scene, rd)])
+    b = pb.Batch([(scene, rd)], best)
+    tuned_ms = timed(b.run)
+    rays = b.rays_traced()
+    tuned_film, tuned_prim = b.output(0)
+    b.close()
+    res = {"workload": "instanced displaced spheres (5 x 1,310,720 + 2 tris), 1920x1080, 64 spp, depth 8, NEE",
+           "samples": samples, "rays": int(rays),
+           "plain": {"ms": round(plain_ms, 2), "msamples_s": round(samples / plain_ms / 1e3, 1), "mrays_s": round(rays / plain_ms / 1e3, 1)},
+           "autotuned": {"ms": round(tuned_ms, 2), "msamples_s": round(samples / tuned_ms / 1e3, 1),
+                         "mrays_s": round(rays / tuned_ms / 1e3, 1), "tuning": best.as_dict(), "trials": len(trials)},
+           "autotuned_equals_plain": bool(np.array_equal(tuned_film.view(np.uint32), film.view(np.uint32))
+                                          and np.array_equal(tuned_prim, prim_ids)),
+           "timing": "CUDA events, median of 3 after one warm-up; films stay on the device"}
+    if cpu:
+        from oracle import pyoracle as po
+        threads = threads or os.cpu_count() or 1
+        kind = "reference" if po.ref_available() else "port"
+        cpu_scene = po.RefScene(meshes, env) if kind == "reference" else po.OracleScene(meshes, env)
+        r0 = rd.height // 2 - cpu_rows // 2
+        desc = dict(d, flags=pb.RENDER_NEE)
+        t0 = time.perf_counter()
+        ref_rgb, ref_prim = cpu_scene.render(desc, rows=(r0, r0 + cpu_rows), threads=threads)
+        dt = time.perf_counter() - t0
+        a = film[r0:r0 + cpu_rows].astype(np.float64)
+        r = ref_rgb[r0:r0 + cpu_rows].astype(np.float64)
+        rmse = float(np.sqrt(np.mean((a - r) ** 2)) / max(np.sqrt(np.mean(r ** 2)), 1e-30))
+        res["vs_cpu"] = {"kind": kind, "rows": [int(r0), int(r0 + cpu_rows)], "rel_rmse": rmse,
+                         "mean_abs_pixel_error": float(np.mean(np.abs(a - r))),
+                         "bit_exact": bool(np.array_equal(film[r0:r0 + cpu_rows].view(np.uint32), ref_rgb[r0:r0 + cpu_rows].view(np.uint32))),
+                         "primary_ids_equal": bool(np.array_equal(prim_ids[r0:r0 + cpu_rows], ref_prim[r0:r0 + cpu_rows])),
+                         "cpu_msamples_s": round(rd.width * cpu_rows * rd.spp / dt / 1e6, 4), "cores": threads}
+        cpu_scene.close()
+    scene.close()
+    return res
+
+
+def serve_requests(pb, n_scenes, n_requests, seed):
+    """The request mix of the serving workload: scene uniform, resolution in {128..1024}^2, spp in
+    {1, 4, 16}, depth 5, next-event estimation on."""
+    from polytope_b200 import workloads as W
     rng = np.random.default_rng(seed)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    unit_arrivals = np.cumsum(rng.exponential(1.0, n_requests))  # divided by the rate
     reqs = []
     for k in range(n_requests):
         res = int(rng.choice([128, 256, 512, 1024]))
         spp = int(rng.choice([1, 4, 16]))
         reqs.append((int(rng.integers(n_scenes)), pb.render_desc(res, res, spp, 5, W.SERVE_CAMERA, k + 1, pb.RENDER_NEE)))
+    return reqs, unit_arrivals
 
-    def run_served():
-        srv = pb.Server(max_inflight=64, wave_pixels=1 << 22, tuning=pb.default_tuning())
-        t0 = time.perf_counter()
-        tickets = []
-        for (si, rd), at in zip(reqs, arrivals):
-            now = time.perf_counter() - t0
-            if at > now:
-                time.sleep(at - now)
-            tickets.append(srv.submit(scenes[si], rd))
-        lats = []
-        for t in tickets:
-            srv.wait(t, 600000)
-            lats.append(srv.poll(t)[1])
-            srv.fetch(t)
-        span = time.perf_counter() - t0
-        rays = srv.stats()["rays_traced"]
-        srv.close()
-        return np.array(lats), span, rays
 
-    def run_plain():
-        done = [0.0] * n_requests
-        t0 = time.perf_counter()
+def serve_tuning(pb):
+    t = pb.default_tuning()
+    t.pipeline = pb.PIPELINE_PATHS
+    return t
 
-        def worker():
-            for k, (si, rd) in enumerate(reqs):
-                now = time.perf_counter() - t0
-                if arrivals[k] > now:
-                    time.sleep(arrivals[k] - now)
-                rgb = np.empty((rd.height, rd.width, 3), np.float32)
-                pb.check(pb.lib.pt_render(scenes[si].handle, ctypes.byref(rd), rgb.ctypes.data, None, 0, None))
-                done[k] = time.perf_counter() - t0
-        th = threading.Thread(target=worker)
-        th.start()
-        th.join()
-        return np.array(done) - arrivals, time.perf_counter() - t0
 
-    lat_s, span_s, rays = run_served()
-    lat_p, span_p = run_plain()
-    lat_p = lat_p * 1000.0
+def run_served(pb, scenes, reqs, arrivals, wave=1 << 23, policy=0, tuning=None):
+    """Submits each request at its arrival time; returns (latencies ms, makespan s, rays)."""
+    srv = pb.Server(max_inflight=64, wave_pixels=wave, tuning=tuning or serve_tuning(pb), policy=policy)
+    t0 = time.perf_counter()
+    tickets = []
+    for (si, rd), at in zip(reqs, arrivals):
+        now = time.perf_counter() - t0
+        if at > now:
+            time.sleep(at - now)
+        tickets.append(srv.submit(scenes[si], rd))
+    lats = []
+    for t in tickets:
+        srv.wait(t, 600000)
+        lats.append(srv.poll(t)[1])
+        srv.fetch(t)
+    span = time.perf_counter() - t0
+    rays = srv.stats()["rays_traced"]
+    srv.close()
+    return np.array(lats), span, rays
+
+
+def run_plain(pb, scenes, reqs, arrivals):
+    """One pt_render per request in arrival order (host film out); returns (latencies ms, makespan s)."""
+    done = np.zeros(len(reqs))
+    t0 = time.perf_counter()
+    for k, (si, rd) in enumerate(reqs):
+        now = time.perf_counter() - t0
+        if arrivals[k] > now:
+            time.sleep(arrivals[k] - now)
+        rgb = np.empty((rd.height, rd.width, 3), np.float32)
+        pb.check(pb.lib.pt_render(scenes[si].handle, ctypes.byref(rd), rgb.ctypes.data, None, 0, None))
+        done[k] = time.perf_counter() - t0
+    return (done - arrivals) * 1000.0, time.perf_counter() - t0
+
+
+def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 2000.0), seed=19):
+    """Resident scene pool, Poisson request arrivals at each rate: the serving loop vs one
+    pt_render per request in arrival order.  Latency = completion - arrival."""
+    from polytope_b200 import workloads as W
+    scenes = build_scenes(pb, W.serving_pool(n_scenes))
+    reqs, unit = serve_requests(pb, n_scenes, n_requests, seed)
+    warm = reqs[:8]
+    run_served(pb, scenes, warm, np.zeros(len(warm)))
+    run_plain(pb, scenes, warm, np.zeros(len(warm)))
     pct = lambda a, q: round(float(np.percentile(a, q)), 2)
-    return {"workload": f"{n_scenes} resident scenes (instanced displaced spheres, 100k-4M tris), {n_requests} Poisson requests at {rate:g}/s, 128^2-1024^2, 1/4/16 spp, depth 5",
-            "rays": int(rays),
-            "served": {"mrays_s": round(rays / span_s / 1e6, 1), "p50_ms": pct(lat_s, 50), "p95_ms": pct(lat_s, 95), "p99_ms": pct(lat_s, 99), "makespan_s": round(span_s, 3)},
-            "plain_per_request": {"mrays_s": round(rays / span_p / 1e6, 1), "p50_ms": pct(lat_p, 50), "p95_ms": pct(lat_p, 95), "p99_ms": pct(lat_p, 99), "makespan_s": round(span_p, 3)},
-            "timing": "host steady clock from first arrival to last completion; per-request latency = completion - arrival"}
+    out = {"workload": f"{n_scenes} resident scenes (instanced displaced spheres, 100k-4M tris), {n_requests} Poisson requests per rate, "
+                       "128^2-1024^2, 1/4/16 spp, depth 5, NEE",
+           "server": "path-wave pipeline, oldest-first waves of 8,388,608 paths, 2 waves queued",
+           "timing": "host steady clock from the first arrival to the last completion; latency = completion - arrival",
+           "rates": []}
+    for rate in rates:
+        arrivals = unit / rate
+        lat_s, span_s, rays = run_served(pb, scenes, reqs, arrivals)
+        lat_p, span_p = run_plain(pb, scenes, reqs, arrivals)
+        out["rays"] = int(rays)
+        out["rates"].append({
+            "rate_per_s": rate,
+            "served": {"mrays_s": round(rays / span_s / 1e6, 1), "p50_ms": pct(lat_s, 50), "p95_ms": pct(lat_s, 95),
+                       "p99_ms": pct(lat_s, 99), "makespan_s": round(span_s, 3)},
+            "plain_per_request": {"mrays_s": round(rays / span_p / 1e6, 1), "p50_ms": pct(lat_p, 50), "p95_ms": pct(lat_p, 95),
+                                  "p99_ms": pct(lat_p, 99), "makespan_s": round(span_p, 3)}})
+    return out
 
 
 def make_workload(n_rays):
@@ -262,6 +353,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-render", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
 
@@ -372,6 +464,8 @@ def main():
         }
         if not args.no_batched and world == 1:
             line["batched"] = bench_batched(pb, torch)
+        if not args.no_render and world == 1:
+            line["render"] = bench_render(pb, torch, cpu=not args.no_cpu_baseline)
         if not args.no_served and world == 1:
             line["served"] = bench_served(pb, torch)
         if not args.no_cpu_baseline:

@@ -196,6 +196,8 @@ typedef struct pt_camera {
                                      reference CenterSampler, samplers.cpp:13-18)             */
 #define PT_RENDER_WAVEFRONT  4u   /* queue-based wavefront kernels (default: one fused path
                                      kernel per wave)                                         */
+#define PT_RENDER_PERSISTENT 8u   /* one persistent path kernel per wave whose lanes take the
+                                     next path as soon as theirs ends (no PT_RENDER_WAVEFRONT) */
 
 typedef struct pt_render_desc {
     uint32_t  width, height;
@@ -237,7 +239,7 @@ int pt_render_noalloc(pt_scene *scene, const pt_render_desc *desc, float *rgb_de
 /* One render of a batch.  The batch keeps its own device films; read them with pt_batch_output. */
 typedef struct pt_batch_item {
     pt_scene      *scene;
-    pt_render_desc desc;              /* fused pipeline only (no PT_RENDER_WAVEFRONT)             */
+    pt_render_desc desc;              /* no pipeline flags: the batch tuning picks the pipeline  */
 } pt_batch_item;
 
 /* Launch shape of a batch (chosen by pt_batch_autotune).
@@ -245,9 +247,13 @@ typedef struct pt_batch_item {
  *                          takes the next pixel of any render (wave_pixels: pixels per launch).
  *   PT_PIPELINE_WAVEFRONT: waves of paths of all renders; per bounce a persistent extend kernel,
  *                          a shade kernel appending to ray / shadow queues, a persistent shadow
- *                          kernel (wave_pixels: paths per wave). */
+ *                          kernel (wave_pixels: paths per wave).
+ *   PT_PIPELINE_PATHS:     waves of paths of all renders as in PT_PIPELINE_WAVEFRONT, but one
+ *                          thread runs a whole path (pt_render's fused kernel over several
+ *                          renders at once; wave_pixels: paths per wave). */
 #define PT_PIPELINE_FUSED     0u
 #define PT_PIPELINE_WAVEFRONT 1u
+#define PT_PIPELINE_PATHS     2u
 typedef struct pt_batch_tuning {
     uint64_t wave_pixels;             /* work per launch / wave; 0 = automatic                    */
     uint32_t threads_per_block;       /* 64, 128 or 256                                           */
@@ -284,11 +290,16 @@ int pt_batch_autotune(const pt_batch_item *items, uint32_t n, pt_batch_tuning *b
 
 /* ---- serving loop (continuous batching of render requests over resident scenes) ----------- */
 
+/* Wave policies of the serving loop. */
+#define PT_SERVE_OLDEST_FIRST 0u  /* each wave is filled from the oldest admitted requests first      */
+#define PT_SERVE_FAIR_SHARE   1u  /* each wave gives every admitted request an equal share            */
+
 typedef struct pt_server_config {
     uint32_t        max_inflight;     /* requests admitted at once                                 */
     uint64_t        memory_budget;    /* device bytes for admitted requests' films (0 = 80 % free) */
-    uint64_t        wave_pixels;      /* pixels per wave, shared fairly by admitted requests       */
+    uint64_t        wave_pixels;      /* work per wave: pixels (PT_PIPELINE_FUSED) or paths (others) */
     pt_batch_tuning tuning;
+    uint32_t        policy;           /* PT_SERVE_OLDEST_FIRST or PT_SERVE_FAIR_SHARE              */
 } pt_server_config;
 
 typedef struct pt_server_stats {
@@ -300,9 +311,11 @@ typedef struct pt_server_stats {
 typedef struct pt_server pt_server;
 
 /* A scheduler thread admits queued requests while max_inflight and the memory budget allow and
- * runs waves that take a fair share of pixels from every admitted request, so requests arriving
- * while others run join the next wave.  Request states: 0 queued, 1 admitted, 2 done, < 0 error.
- * A request's film is identical to pt_render's whether it ran alone or in any mix. */
+ * runs waves that take work from the admitted requests by the configured policy, so requests
+ * arriving while others run join the next wave.  Two waves stay queued on the GPU while the host
+ * plans the next one and copies finished films out.  Request states: 0 queued, 1 admitted,
+ * 2 done, < 0 error.  A request's film is identical to pt_render's whether it ran alone or in
+ * any mix.  No counterpart in the reference, which renders one frame per process. */
 int pt_server_create(const pt_server_config *cfg, pt_server **out);
 int pt_server_submit(pt_server *server, pt_scene *scene, const pt_render_desc *desc, uint64_t *ticket);
 /* latency_ms: submit to completion (-1 until done). */

@@ -31,7 +31,7 @@ PRIM_NONE = 0xFFFFFFFF
 MAT_LAMBERT, MAT_MIRROR = 1, 2
 RAY_ANY_HIT = 1
 MEM_DEVICE = 1
-RENDER_NEE, RENDER_JITTER, RENDER_WAVEFRONT = 1, 2, 4
+RENDER_NEE, RENDER_JITTER, RENDER_WAVEFRONT, RENDER_PERSISTENT = 1, 2, 4, 8
 
 RAY_DTYPE = np.dtype([("org", "<f4", 3), ("tmax", "<f4"), ("dir", "<f4", 3), ("flags", "<u4")])
 HIT_DTYPE = np.dtype([("prim", "<u4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
@@ -92,7 +92,8 @@ class BatchItem(C.Structure):
     _fields_ = [("scene", _vp), ("desc", RenderDesc)]
 
 
-PIPELINE_FUSED, PIPELINE_WAVEFRONT = 0, 1
+PIPELINE_FUSED, PIPELINE_WAVEFRONT, PIPELINE_PATHS = 0, 1, 2
+SERVE_OLDEST_FIRST, SERVE_FAIR_SHARE = 0, 1
 
 
 class BatchTuning(C.Structure):
@@ -109,7 +110,7 @@ class BatchTuneResult(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("max_inflight", C.c_uint32), ("memory_budget", C.c_uint64), ("wave_pixels", C.c_uint64),
-                ("tuning", BatchTuning)]
+                ("tuning", BatchTuning), ("policy", C.c_uint32)]
 
 
 class ServerStats(C.Structure):
@@ -482,12 +483,13 @@ class Server:
     """Continuous batching of render requests over resident scenes (pt_server_*)."""
 
     def __init__(self, max_inflight: int = 64, memory_budget: int = 0, wave_pixels: int = 1 << 20,
-                 tuning: Optional[BatchTuning] = None):
+                 tuning: Optional[BatchTuning] = None, policy: int = 0):
         cfg = ServerConfig()
         cfg.max_inflight = max_inflight
         cfg.memory_budget = memory_budget
         cfg.wave_pixels = wave_pixels
         cfg.tuning = tuning if tuning is not None else default_tuning()
+        cfg.policy = policy
         h = _vp()
         check(lib.pt_server_create(C.byref(cfg), C.byref(h)))
         self.handle = h

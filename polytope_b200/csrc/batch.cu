@@ -142,7 +142,8 @@ int check_tuning(const pt_batch_tuning& t) {
     if (t.queue_chunk < 32 || t.queue_chunk > 4096 || (t.queue_chunk & 31u))
         return fail(PT_EINVAL, "queue_chunk must be a multiple of 32 in [32, 4096]");
     if (t.stack_depth > PT_TRAVERSAL_STACK) return fail(PT_EINVAL, "stack_depth above the traversal stack limit");
-    if (t.pipeline != PT_PIPELINE_FUSED && t.pipeline != PT_PIPELINE_WAVEFRONT) return fail(PT_EINVAL, "unknown pipeline");
+    if (t.pipeline != PT_PIPELINE_FUSED && t.pipeline != PT_PIPELINE_WAVEFRONT && t.pipeline != PT_PIPELINE_PATHS)
+        return fail(PT_EINVAL, "unknown pipeline");
     return PT_OK;
 }
 
@@ -211,7 +212,8 @@ int wf_build(pt_batch* b, const pt_batch_item* items, const pt_batch_tuning& t) 
     const size_t res_bytes = up(sizeof(WfPixels) * plan.resolve.size());
     const size_t fin_bytes = up(sizeof(WfPixels) * std::max<size_t>(1, plan.finish.size()));
     const size_t tables = item_bytes + seg_bytes + res_bytes + fin_bytes;
-    if (cudaMalloc(&b->wf, film_bytes + tables + wf_state_bytes((uint32_t)wave)) != cudaSuccess)
+    const bool paths = t.pipeline == PT_PIPELINE_PATHS;
+    if (cudaMalloc(&b->wf, film_bytes + tables + wf_state_bytes((uint32_t)wave, paths)) != cudaSuccess)
         return fail(PT_ENOMEM, "cudaMalloc wavefront batch buffers");
     char* base = (char*)b->wf;
     b->wf_films = base;
@@ -220,7 +222,7 @@ int wf_build(pt_batch* b, const pt_batch_item* items, const pt_batch_tuning& t) 
     b->d_segs = (WfSegment*)(base + film_bytes + item_bytes);
     b->d_res = (WfPixels*)(base + film_bytes + item_bytes + seg_bytes);
     b->d_fin = (WfPixels*)(base + film_bytes + item_bytes + seg_bytes + res_bytes);
-    wf_state_carve(base + film_bytes + tables, (uint32_t)wave, b->ws);
+    wf_state_carve(base + film_bytes + tables, (uint32_t)wave, b->ws, paths);
     std::vector<char> host(tables, 0);
     std::vector<WfItem> hi(b->n);
     for (uint32_t i = 0; i < b->n; ++i)
@@ -235,6 +237,7 @@ int wf_build(pt_batch* b, const pt_batch_item* items, const pt_batch_tuning& t) 
     b->wt.threads_per_block = t.threads_per_block;
     b->wt.queue_chunk = t.queue_chunk;
     b->wt.stack_cap = b->cap;
+    b->wt.paths = t.pipeline == PT_PIPELINE_PATHS;
     return PT_OK;
 }
 
@@ -272,7 +275,8 @@ extern "C" int pt_batch_create(const pt_batch_item* items, uint32_t n, const pt_
     for (uint32_t i = 0; i < n; ++i) {
         rc = check_render_desc(items[i].scene, &items[i].desc);
         if (rc) return fail(rc, "batch item " + std::to_string(i) + ": " + pt_last_error());
-        if (items[i].desc.flags & PT_RENDER_WAVEFRONT) return fail(PT_EINVAL, "batch items run the fused pipeline (no PT_RENDER_WAVEFRONT)");
+        if (items[i].desc.flags & (PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT))
+            return fail(PT_EINVAL, "batch items take the batch's pipeline (no PT_RENDER_WAVEFRONT / PT_RENDER_PERSISTENT)");
         if (i && items[i].scene->device != items[0].scene->device) return fail(PT_EINVAL, "batch items on different devices");
         max_depth = std::max(max_depth, items[i].scene->max_depth);
         b->scenes.push_back(items[i].scene);
@@ -314,7 +318,7 @@ extern "C" int pt_batch_create(const pt_batch_item* items, uint32_t n, const pt_
     if (e == cudaSuccess) e = cudaMemcpy(b->items, hi.data(), sizeof(BatchItem) * n, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(PT_ECUDA, std::string("batch setup: ") + cudaGetErrorString(e));
-    if (t.pipeline == PT_PIPELINE_WAVEFRONT) {
+    if (t.pipeline != PT_PIPELINE_FUSED) {
         rc = wf_build(b.get(), items, t);
         if (rc) return rc;
     }
@@ -421,7 +425,8 @@ extern "C" int pt_batch_autotune(const pt_batch_item* items, uint32_t n, pt_batc
     if (results && written < cap_results) results[written++] = pt_batch_tune_result{cur, cur_ms};
     for (int knob = 0; knob < 5; ++knob) {
         std::vector<pt_batch_tuning> cands;
-        if (knob == 0) for (uint32_t v : {PT_PIPELINE_FUSED, PT_PIPELINE_WAVEFRONT}) { auto c = cur; c.pipeline = v; cands.push_back(c); }
+        if (knob == 0)
+            for (uint32_t v : {PT_PIPELINE_FUSED, PT_PIPELINE_WAVEFRONT, PT_PIPELINE_PATHS}) { auto c = cur; c.pipeline = v; cands.push_back(c); }
         if (knob == 1) for (uint32_t v : {64u, 128u, 256u}) { auto c = cur; c.threads_per_block = v; cands.push_back(c); }
         if (knob == 2) for (uint32_t v : {32u, 64u, 128u, 256u}) { auto c = cur; c.queue_chunk = v; cands.push_back(c); }
         if (knob == 3) for (uint32_t v : {24u, 32u, 48u, 64u}) { if (v < max_depth + 2) continue; auto c = cur; c.stack_depth = v; cands.push_back(c); }

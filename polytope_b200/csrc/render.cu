@@ -11,8 +11,10 @@
 
 #include <algorithm>
 #include <cstring>
+#include <mutex>
 #include <string>
 
+#include "batch.h"
 #include "launch.h"
 #include "pt_internal.h"
 #include "render.h"
@@ -84,9 +86,51 @@ cudaError_t launch_finish_film(const float* film, uint32_t npix, uint32_t spp, f
 using namespace pt;
 
 namespace {
+// Temporaries of a render come from a stream-ordered pool per device, owned by the library, that
+// keeps up to 2 GiB cached between calls.  A cudaMalloc / cudaFree pair per frame synchronises
+// the whole device on every call, and on a device holding tens of GB of resident scenes single
+// frees were seen to stall for 0.1-1 s.
+cudaMemPool_t render_pool(int device) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    if (device < 0 || device >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[device]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = 2ull << 30;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[device] = p;
+    }
+    return pools[device];
+}
+
 struct DevBuf {
     void* p = nullptr;
-    ~DevBuf() { if (p) cudaFree(p); }
+    cudaStream_t s = nullptr;
+    bool pooled = false;
+    // Stream-ordered on `st` from `pool` (plain cudaMalloc if the pool could not be made).
+    bool alloc(size_t n, cudaMemPool_t pool, cudaStream_t st) {
+        s = st;
+        pooled = pool != nullptr;
+        const cudaError_t e = pooled ? cudaMallocFromPoolAsync(&p, n, pool, st) : cudaMalloc(&p, n);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            p = nullptr;
+        }
+        return p != nullptr;
+    }
+    ~DevBuf() {
+        if (!p) return;
+        if (pooled) cudaFreeAsync(p, s); else cudaFree(p);
+    }
 };
 }  // namespace
 
@@ -122,8 +166,10 @@ int check_render_desc(const pt_scene* s, const pt_render_desc* desc) {
     if ((uint64_t)desc->width * desc->height > (1u << 30)) return fail(PT_EINVAL, "frame too large");
     if ((uint64_t)desc->width * desc->height * desc->spp > (1ull << 40)) return fail(PT_EINVAL, "too many samples");
     if (desc->max_depth > 1024) return fail(PT_EINVAL, "max_depth above 1024");
-    if (desc->flags & ~(uint32_t)(PT_RENDER_NEE | PT_RENDER_JITTER | PT_RENDER_WAVEFRONT))
+    if (desc->flags & ~(uint32_t)(PT_RENDER_NEE | PT_RENDER_JITTER | PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT))
         return fail(PT_EINVAL, "unknown render flags");
+    if ((desc->flags & PT_RENDER_WAVEFRONT) && (desc->flags & PT_RENDER_PERSISTENT))
+        return fail(PT_EINVAL, "PT_RENDER_WAVEFRONT and PT_RENDER_PERSISTENT exclude each other");
     if ((int)s->max_depth + 2 > PT_TRAVERSAL_STACK) return fail(PT_ESTACK, "tree too deep for the traversal stack");
     return PT_OK;
 }
@@ -142,29 +188,32 @@ extern "C" int pt_render(pt_scene* s, const pt_render_desc* desc, float* rgb_out
     struct Restore { int d; ~Restore() { if (d >= 0) cudaSetDevice(d); } } restore{prev != s->device ? prev : -1};
 
     const RenderParams p = render_params(s, desc);
-    const bool wavefront = (desc->flags & PT_RENDER_WAVEFRONT) != 0;
+    // the wave engine runs both the queue-based kernels and the persistent path kernel
+    const bool persistent = (desc->flags & PT_RENDER_PERSISTENT) != 0;
+    const bool wavefront = (desc->flags & PT_RENDER_WAVEFRONT) != 0 || persistent;
     cudaStream_t st = (cudaStream_t)stream;
     const uint64_t total = npix64 * desc->spp;
     uint32_t wave = desc->wave_paths ? desc->wave_paths : (wavefront ? (1u << 22) : (1u << 22));
     if (wave > total) wave = (uint32_t)total;
+    cudaMemPool_t pool = render_pool(s->device);
     DevBuf rad, film, rgb_dev, prim_dev, wsbuf, tables;
-    if ((!wavefront && cudaMalloc(&rad.p, 12 * (size_t)wave) != cudaSuccess) || cudaMalloc(&film.p, 12 * (size_t)npix) != cudaSuccess)
-        return fail(PT_ENOMEM, "cudaMalloc render buffers");
+    if ((!wavefront && !rad.alloc(12 * (size_t)wave, pool, st)) || !film.alloc(12 * (size_t)npix, pool, st))
+        return fail(PT_ENOMEM, "device memory for the render buffers");
     WfState ws{};
     WfPlan plan;
     if (wavefront) {
-        if (cudaMalloc(&wsbuf.p, wf_state_bytes(wave)) != cudaSuccess) return fail(PT_ENOMEM, "cudaMalloc wavefront queues");
-        wf_state_carve(wsbuf.p, wave, ws);
+        if (!wsbuf.alloc(wf_state_bytes(wave, persistent), pool, st)) return fail(PT_ENOMEM, "device memory for the wavefront queues");
+        wf_state_carve(wsbuf.p, wave, ws, persistent);
         wf_plan_all(plan, {npix}, {desc->spp}, {desc->max_depth}, wave);
     }
     const bool dev_out = (mem_flags & PT_MEM_DEVICE) != 0;
     float* rgb_d = rgb_out;
     uint32_t* prim_d = primary_out;
     if (!dev_out) {
-        if (cudaMalloc(&rgb_dev.p, 12 * (size_t)npix) != cudaSuccess) return fail(PT_ENOMEM, "cudaMalloc film");
+        if (!rgb_dev.alloc(12 * (size_t)npix, pool, st)) return fail(PT_ENOMEM, "device memory for the film");
         rgb_d = (float*)rgb_dev.p;
         if (primary_out) {
-            if (cudaMalloc(&prim_dev.p, 4 * (size_t)npix) != cudaSuccess) return fail(PT_ENOMEM, "cudaMalloc prim");
+            if (!prim_dev.alloc(4 * (size_t)npix, pool, st)) return fail(PT_ENOMEM, "device memory for the primary ids");
             prim_d = (uint32_t*)prim_dev.p;
         }
     }
@@ -177,8 +226,8 @@ extern "C" int pt_render(pt_scene* s, const pt_render_desc* desc, float* rgb_out
         const size_t sbytes = ((sizeof(WfSegment) * plan.segments.size()) + 255) & ~(size_t)255;
         const size_t rbytes = ((sizeof(WfPixels) * plan.resolve.size()) + 255) & ~(size_t)255;
         const size_t fbytes = sizeof(WfPixels) * plan.finish.size();
-        if (cudaMalloc(&tables.p, pbytes + ibytes + sbytes + rbytes + fbytes) != cudaSuccess)
-            return fail(PT_ENOMEM, "cudaMalloc wavefront tables");
+        if (!tables.alloc(pbytes + ibytes + sbytes + rbytes + fbytes, pool, st))
+            return fail(PT_ENOMEM, "device memory for the wavefront tables");
         char* tb = (char*)tables.p;
         RenderParams* d_params = (RenderParams*)tb;
         WfItem* d_item = (WfItem*)(tb + pbytes);
@@ -192,7 +241,8 @@ extern "C" int pt_render(pt_scene* s, const pt_render_desc* desc, float* rgb_out
         if (e == cudaSuccess) e = cudaMemcpyAsync(d_res, plan.resolve.data(), sizeof(WfPixels) * plan.resolve.size(), cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(d_fin, plan.finish.data(), sizeof(WfPixels) * plan.finish.size(), cudaMemcpyHostToDevice, st);
         WfTuning t;
-        t.stack_cap = PT_TRAVERSAL_STACK;
+        t.stack_cap = stack_cap_for(s->max_depth, 0);
+        t.paths = persistent;
         for (size_t k = 0; e == cudaSuccess && k < plan.waves.size(); ++k)
             e = wf_launch_wave(d_item, d_segs, d_res, d_fin, plan.waves[k], ws, t, nullptr, st);
     } else {

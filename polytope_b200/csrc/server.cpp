@@ -2,13 +2,19 @@
 //
 // Scenes stay resident in HBM (pt_scene handles).  Requests (scene, resolution, spp, depth) are
 // queued by pt_server_submit; a scheduler thread admits them while the in-flight limit and the
-// device-memory budget (film + primary ids of each admitted request) allow, and runs waves: each
-// wave takes a fair share of pixels from every admitted request and traces them in one persistent
-// launch of the multi-render kernel (batch.cu), so requests that arrive while others run join the
-// next wave and their work overlaps on the device.  A request completes when its last pixel is
-// done; its film is copied to host memory and its device memory is released for the next
-// admissions.  Pixels are independent and each pixel's samples are summed in sample order, so a
-// request's film is bit-identical whether it ran alone or in any mix.
+// device-memory budget (film + primary ids of each admitted request) allow, and plans waves: a
+// wave takes work (paths for the wavefront pipeline, pixels for the fused one) from the admitted
+// requests, oldest first (PT_SERVE_OLDEST_FIRST) or a fair share from each (PT_SERVE_FAIR_SHARE),
+// and traces it in one multi-render launch sequence, so requests that arrive while others run
+// join the next wave and their work overlaps on the device.
+//
+// Two waves are kept queued on the stream: while the GPU runs wave k the host plans and enqueues
+// wave k+1, then retires wave k.  The films of the requests that finish in a wave are copied to
+// pinned host blocks on a second stream right behind the wave's kernels, so the copies overlap the
+// next wave; retiring waits for those copies and releases the requests' device memory, which is
+// stream-ordered, so no call here synchronises the whole device.  Pixels are independent and
+// each pixel's samples are summed in sample order, so a request's film is bit-identical whether
+// it ran alone or in any mix.
 
 #include <algorithm>
 #include <chrono>
@@ -32,21 +38,22 @@ using Clock = std::chrono::steady_clock;
 
 namespace {
 
+constexpr int kWavesQueued = 2;  // waves enqueued on the stream at once (host planning overlaps the GPU)
+
 struct Request {
     uint64_t ticket = 0;
     pt_scene* scene = nullptr;
     pt_render_desc desc{};
     pt::RenderParams params{};
     uint32_t npix = 0;
-    uint32_t next_px = 0;         // fused pipeline: pixels done
-    uint64_t next_path = 0;       // wavefront pipeline: paths done (sample-major)
-    uint64_t total_paths = 0;
+    uint64_t total = 0;           // work units: pixels (fused) or paths (wavefront, sample-major)
+    uint64_t planned = 0;         // units handed to waves so far
     size_t bytes = 0;
     void* dev = nullptr;          // RenderParams, rgb (3 floats/px), primary ids, film sums (wavefront)
     int state = 0;                // 0 queued, 1 admitted, 2 done, < 0 error
     Clock::time_point submitted, done;
-    std::vector<float> rgb;
-    std::vector<uint32_t> prim;
+    void* host = nullptr;         // pinned block: rgb (3 floats/px) then primary ids, once finished
+    size_t host_bytes = 0;        // the block's size class
 };
 
 static_assert(sizeof(pt::RenderParams) <= 256, "request layout reserves 256 bytes for the parameters");
@@ -59,6 +66,57 @@ float* req_rgb(const Request* r) { return (float*)((char*)r->dev + 256); }
 uint32_t* req_prim(const Request* r) { return (uint32_t*)((char*)r->dev + 256 + up256(12 * (size_t)r->npix)); }
 float* req_film(const Request* r) { return (float*)((char*)r->dev + 256 + up256(12 * (size_t)r->npix) + up256(4 * (size_t)r->npix)); }
 
+// Pinned host blocks for finished films, cached by power-of-two size class: page-locking memory is
+// slow, and copies into pinned memory run at full link speed.
+class PinnedCache {
+  public:
+    void* get(size_t bytes, size_t& cls) {
+        cls = 1u << 16;
+        while (cls < bytes) cls <<= 1;
+        auto& v = free_[cls];
+        if (!v.empty()) {
+            void* p = v.back();
+            v.pop_back();
+            cached_ -= cls;
+            return p;
+        }
+        void* p = nullptr;
+        if (cudaMallocHost(&p, cls) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return p;
+    }
+    void put(void* p, size_t cls) {
+        if (!p) return;
+        if (cached_ + cls > kMaxCached) {
+            cudaFreeHost(p);
+            return;
+        }
+        free_[cls].push_back(p);
+        cached_ += cls;
+    }
+    void clear() {
+        for (auto& kv : free_)
+            for (void* p : kv.second) cudaFreeHost(p);
+        free_.clear();
+        cached_ = 0;
+    }
+
+  private:
+    static constexpr size_t kMaxCached = 1ull << 30;
+    std::unordered_map<size_t, std::vector<void*>> free_;
+    size_t cached_ = 0;
+};
+
+// A wave enqueued on the stream and not yet retired.
+struct WaveInFlight {
+    int slot = 0;                      // staging / event slot
+    cudaError_t launch = cudaSuccess;  // error from enqueueing it
+    std::vector<Request*> members;     // requests with work in this wave
+    std::vector<Request*> finishing;   // requests whose last work unit is in this wave
+};
+
 }  // namespace
 
 struct pt_server {
@@ -69,20 +127,25 @@ struct pt_server {
     std::condition_variable cv;       // new work or stop
     std::condition_variable done_cv;  // a request finished
     std::deque<Request*> pending;
-    std::vector<Request*> active;
+    std::vector<Request*> active;     // admission order
     std::unordered_map<uint64_t, std::unique_ptr<Request>> all;
     bool stop = false;
     uint64_t next_ticket = 1;
     size_t mem_in_use = 0;
     std::string worker_error;
     // device / pinned resources of the scheduler
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;       // waves
+    cudaStream_t copy_stream = nullptr;  // film copies to host
+    cudaMemPool_t pool = nullptr;        // request memory (stream-ordered)
+    cudaEvent_t ev_start[kWavesQueued] = {}, ev_end[kWavesQueued] = {}, ev_copied[kWavesQueued] = {};
+    PinnedCache pinned;                  // guarded by mu
     void* d_items = nullptr;
-    pt::BatchItem* h_items = nullptr;  // pinned
-    void* d_counters = nullptr;        // ray counter, rays traced
+    pt::BatchItem* h_items = nullptr;    // pinned, kWavesQueued * max_items
+    void* d_counters = nullptr;          // [0] fetch counter of the fused launch, [1] rays traced (cumulative)
+    unsigned long long* h_rays = nullptr;  // pinned, one per slot
     uint32_t max_items = 0;
-    // wavefront pipeline: wave state and per-wave tables (device + pinned staging)
-    bool wavefront = false;
+    // wavefront pipeline: wave state and per-wave tables (device + pinned staging per slot)
+    bool wavefront = false;              // work in paths through the wave engine (PT_PIPELINE_WAVEFRONT / _PATHS)
     void* d_wave = nullptr;
     pt::WfState ws{};
     void* d_tables = nullptr;
@@ -93,168 +156,278 @@ struct pt_server {
     double busy_ms = 0.0;
 
     void run();
+    void admit();
+    void plan(WaveInFlight& w, std::vector<uint32_t>& take, std::vector<uint64_t>& first);
+    cudaError_t enqueue(WaveInFlight& w, const std::vector<uint32_t>& take, const std::vector<uint64_t>& first);
+    void retire(WaveInFlight& w);
+    void release(Request* r);  // with mu held
+    bool has_unplanned() const {
+        for (const Request* r : active)
+            if (r->state == 1 && r->planned < r->total) return true;
+        return false;
+    }
 };
+
+// Admits queued requests in arrival order while the in-flight limit and the memory budget allow
+// (mu held).  With an empty active set one request is always tried, so a request larger than the
+// budget still runs alone.
+void pt_server::admit() {
+    if (pending.empty()) return;
+    size_t budget = cfg.memory_budget;
+    if (!budget) {
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        uint64_t reserved = 0, used = 0;
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+        budget = (size_t)(0.8 * (double)(free_b + (reserved > used ? reserved - used : 0))) + mem_in_use;
+    }
+    while (!pending.empty() && active.size() < cfg.max_inflight) {
+        Request* r = pending.front();
+        const size_t need = request_bytes(r->npix, wavefront);
+        if (mem_in_use + need > budget && !active.empty()) break;
+        if (cudaMallocFromPoolAsync(&r->dev, need, pool, stream) != cudaSuccess) {
+            cudaGetLastError();
+            r->dev = nullptr;
+            if (!active.empty()) break;  // wait for memory to free up
+            r->state = PT_ENOMEM;
+            pending.pop_front();
+            done_cv.notify_all();
+            continue;
+        }
+        r->bytes = need;
+        mem_in_use += need;
+        r->params.rays_traced = nullptr;
+        cudaMemcpyAsync(r->dev, &r->params, sizeof(r->params), cudaMemcpyHostToDevice, stream);
+        if (wavefront) cudaMemsetAsync(req_film(r), 0, 12 * (size_t)r->npix, stream);
+        r->state = 1;
+        pending.pop_front();
+        active.push_back(r);
+    }
+}
+
+// Picks the next wave's work (mu held): oldest admitted request first, each taking what it has
+// left up to the wave's room, or an equal share of the wave for every request.
+void pt_server::plan(WaveInFlight& w, std::vector<uint32_t>& take, std::vector<uint64_t>& first) {
+    uint64_t room = wavefront ? std::min<uint64_t>(cfg.wave_pixels, ws.capacity) : cfg.wave_pixels;
+    uint64_t share = room;
+    if (cfg.policy == PT_SERVE_FAIR_SHARE) {
+        size_t open = 0;
+        for (const Request* r : active) open += r->state == 1 && r->planned < r->total;
+        if (open) share = std::max<uint64_t>(1024, room / open);
+    }
+    for (Request* r : active) {
+        if (w.members.size() >= max_items || room == 0) break;
+        if (r->state != 1 || r->planned >= r->total) continue;
+        const uint64_t t = std::min<uint64_t>(std::min<uint64_t>(share, r->total - r->planned), room);
+        room -= t;
+        w.members.push_back(r);
+        take.push_back((uint32_t)t);
+        first.push_back(r->planned);
+        r->planned += t;
+        if (r->planned == r->total) w.finishing.push_back(r);
+    }
+}
+
+// Enqueues the wave's tables and kernels on the stream, then the rays-traced read-back and the
+// wave's end event.
+cudaError_t pt_server::enqueue(WaveInFlight& w, const std::vector<uint32_t>& take, const std::vector<uint64_t>& first) {
+    uint32_t max_depth = 0;
+    for (Request* r : w.members) max_depth = std::max(max_depth, r->scene->max_depth);
+    const int cap = pt::stack_cap_for(max_depth, cfg.tuning.stack_depth);
+    unsigned long long* rays = (unsigned long long*)d_counters + 1;
+    cudaError_t e = cudaEventRecord(ev_start[w.slot], stream);
+    if (!wavefront) {
+        pt::BatchItem* hi = h_items + (size_t)w.slot * max_items;
+        uint64_t base = 0;
+        for (size_t i = 0; i < w.members.size(); ++i) {
+            Request* r = w.members[i];
+            pt::BatchItem& it = hi[i];
+            it.params = (const pt::RenderParams*)r->dev;
+            it.rgb = req_rgb(r);
+            it.primary = req_prim(r);
+            it.px_begin = (uint32_t)first[i];
+            it.px_count = take[i];
+            it.base = base;
+            base += take[i];
+        }
+        // d_items is shared by the queued waves: this copy is stream-ordered after the previous
+        // wave's kernel, its last reader.
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_items, hi, sizeof(pt::BatchItem) * w.members.size(), cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess)
+            e = pt::launch_batch((const pt::BatchItem*)d_items, (uint32_t)w.members.size(), 0, base,
+                                 (unsigned long long*)d_counters, cfg.tuning, cap, rays, stream);
+    } else {
+        // one segment of consecutive paths per request; tables through this slot's pinned staging
+        pt::WfPlan plan;
+        std::vector<pt::WfSegment> segs;
+        std::vector<uint32_t> npix, spp, depth;
+        std::vector<pt::WfItem> witems;
+        uint64_t slot = 0;
+        for (size_t i = 0; i < w.members.size(); ++i) {
+            Request* r = w.members[i];
+            witems.push_back(pt::WfItem{(const pt::RenderParams*)r->dev, req_film(r), req_rgb(r), req_prim(r), r->npix, r->desc.spp});
+            npix.push_back(r->npix);
+            spp.push_back(r->desc.spp);
+            depth.push_back(r->desc.max_depth);
+            segs.push_back(pt::WfSegment{(uint32_t)i, 0, first[i], slot, take[i]});
+            slot += take[i];
+        }
+        pt::wf_add_wave(plan, segs, npix, spp, depth);
+        const size_t ib = up256(sizeof(pt::WfItem) * witems.size()), sb = up256(sizeof(pt::WfSegment) * plan.segments.size());
+        const size_t rb = up256(sizeof(pt::WfPixels) * plan.resolve.size());
+        char* ht = h_tables + (size_t)w.slot * table_bytes;
+        std::memcpy(ht, witems.data(), sizeof(pt::WfItem) * witems.size());
+        std::memcpy(ht + ib, plan.segments.data(), sizeof(pt::WfSegment) * plan.segments.size());
+        std::memcpy(ht + ib + sb, plan.resolve.data(), sizeof(pt::WfPixels) * plan.resolve.size());
+        std::memcpy(ht + ib + sb + rb, plan.finish.data(), sizeof(pt::WfPixels) * plan.finish.size());
+        const size_t used = ib + sb + rb + sizeof(pt::WfPixels) * plan.finish.size();
+        // the device tables are shared by the queued waves, like d_items above
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_tables, ht, used, cudaMemcpyHostToDevice, stream);
+        pt::WfTuning wt;
+        wt.threads_per_block = cfg.tuning.threads_per_block;
+        wt.queue_chunk = cfg.tuning.queue_chunk;
+        wt.stack_cap = cap;
+        wt.paths = cfg.tuning.pipeline == PT_PIPELINE_PATHS;
+        char* dt = (char*)d_tables;
+        if (e == cudaSuccess)
+            e = pt::wf_launch_wave((const pt::WfItem*)dt, (const pt::WfSegment*)(dt + ib), (const pt::WfPixels*)(dt + ib + sb),
+                                   (const pt::WfPixels*)(dt + ib + sb + rb), plan.waves[0], ws, wt, rays, stream);
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h_rays + w.slot, rays, 8, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ev_end[w.slot], stream);
+    // films of the requests this wave finishes: device -> pinned, behind the wave's kernels
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(copy_stream, ev_end[w.slot], 0);
+    for (Request* r : w.finishing) {
+        if (e != cudaSuccess) break;
+        const size_t n = r->npix;
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            r->host = pinned.get(16 * n, r->host_bytes);
+        }
+        if (!r->host) {
+            e = cudaErrorMemoryAllocation;
+            break;
+        }
+        e = cudaMemcpyAsync(r->host, req_rgb(r), 12 * n, cudaMemcpyDeviceToHost, copy_stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync((char*)r->host + 12 * n, req_prim(r), 4 * n, cudaMemcpyDeviceToHost, copy_stream);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ev_copied[w.slot], copy_stream);
+    return e;
+}
+
+// Frees a request's device memory after everything queued so far on the stream and drops it
+// from the active set (mu held).
+void pt_server::release(Request* r) {
+    if (r->dev) {
+        cudaFreeAsync(r->dev, stream);
+        r->dev = nullptr;
+        mem_in_use -= r->bytes;
+    }
+    r->done = Clock::now();
+    active.erase(std::remove(active.begin(), active.end(), r), active.end());
+    ++completed;
+}
+
+// Waits for a wave and for the copies of the films it finished, then releases those requests.
+void pt_server::retire(WaveInFlight& w) {
+    cudaError_t e = w.launch;
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev_copied[w.slot]);
+    float ms = 0.f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, ev_start[w.slot], ev_end[w.slot]);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        busy_ms += ms;
+        ++waves;
+        if (e == cudaSuccess) {
+            rays_traced = h_rays[w.slot];
+            for (Request* r : w.finishing) {
+                if (r->state != 1) continue;
+                r->state = 2;
+                release(r);
+            }
+        } else {
+            worker_error = std::string("serving wave: ") + cudaGetErrorString(e);
+            for (Request* r : w.members) {
+                if (r->state == 1) r->state = PT_ECUDA;
+                if (r->dev || std::find(active.begin(), active.end(), r) != active.end()) release(r);
+            }
+        }
+    }
+    done_cv.notify_all();
+}
 
 void pt_server::run() {
     cudaSetDevice(device);
-    std::vector<Request*> wave_reqs;
-    std::vector<uint32_t> wave_take;
+    std::deque<WaveInFlight> queued;
+    int next_slot = 0;
+    std::vector<uint32_t> take;
+    std::vector<uint64_t> first;
     while (true) {
+        WaveInFlight w;
+        take.clear();
+        first.clear();
+        bool stopping;
         {
             std::unique_lock<std::mutex> lock(mu);
-            cv.wait(lock, [&] { return stop || !pending.empty() || !active.empty(); });
-            if (stop) return;
-            // admission: in-flight limit and device-memory budget
-            size_t free_b = 0, total_b = 0;
-            cudaMemGetInfo(&free_b, &total_b);
-            while (!pending.empty() && active.size() < cfg.max_inflight) {
-                Request* r = pending.front();
-                const size_t need = request_bytes(r->npix, wavefront);
-                const size_t budget = cfg.memory_budget ? cfg.memory_budget : (size_t)(0.8 * (double)free_b) + mem_in_use;
-                if (mem_in_use + need > budget && !active.empty()) break;
-                if (cudaMalloc(&r->dev, need) != cudaSuccess) {
-                    cudaGetLastError();
-                    if (!active.empty()) break;  // wait for memory to free up
-                    r->state = PT_ENOMEM;
-                    pending.pop_front();
-                    done_cv.notify_all();
-                    continue;
-                }
-                r->bytes = need;
-                mem_in_use += need;
-                r->params.rays_traced = nullptr;
-                cudaMemcpyAsync(r->dev, &r->params, sizeof(r->params), cudaMemcpyHostToDevice, stream);
-                if (wavefront) cudaMemsetAsync(req_film(r), 0, 12 * (size_t)r->npix, stream);
-                r->state = 1;
-                pending.pop_front();
-                active.push_back(r);
-            }
-            // one wave: a fair share of pixels from every admitted request
-            wave_reqs.clear();
-            wave_take.clear();
-            if (!active.empty()) {
-                const uint64_t share = std::max<uint64_t>(1024, cfg.wave_pixels / active.size());
-                uint64_t room = wavefront ? ws.capacity : ~0ull;
-                for (Request* r : active) {
-                    if (wave_reqs.size() >= max_items || room == 0) break;
-                    const uint64_t left = wavefront ? r->total_paths - r->next_path : (uint64_t)(r->npix - r->next_px);
-                    const uint32_t take = (uint32_t)std::min<uint64_t>(std::min<uint64_t>(share, left), room);
-                    if (!take) continue;
-                    if (wavefront) room -= take;
-                    wave_reqs.push_back(r);
-                    wave_take.push_back(take);
-                }
+            if (queued.empty()) cv.wait(lock, [&] { return stop || !pending.empty() || has_unplanned(); });
+            stopping = stop;
+            if (!stopping) {
+                admit();
+                plan(w, take, first);
             }
         }
-        if (wave_reqs.empty()) continue;
-        uint32_t max_depth = 0;
-        for (Request* r : wave_reqs) max_depth = std::max(max_depth, r->scene->max_depth);
-        const auto t0 = Clock::now();
-        const int cap = pt::stack_cap_for(max_depth, cfg.tuning.stack_depth);
-        cudaError_t e = cudaMemsetAsync((unsigned long long*)d_counters + 1, 0, 8, stream);
-        if (!wavefront) {
-            uint64_t base = 0;
-            for (size_t i = 0; i < wave_reqs.size(); ++i) {
-                Request* r = wave_reqs[i];
-                pt::BatchItem& it = h_items[i];
-                it.params = (const pt::RenderParams*)r->dev;
-                it.rgb = req_rgb(r);
-                it.primary = req_prim(r);
-                it.px_begin = r->next_px;
-                it.px_count = wave_take[i];
-                it.base = base;
-                base += wave_take[i];
-            }
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(d_items, h_items, sizeof(pt::BatchItem) * wave_reqs.size(), cudaMemcpyHostToDevice, stream);
-            if (e == cudaSuccess)
-                e = pt::launch_batch((const pt::BatchItem*)d_items, (uint32_t)wave_reqs.size(), 0, base,
-                                     (unsigned long long*)d_counters, cfg.tuning, cap, (unsigned long long*)d_counters + 1, stream);
-        } else {
-            // one wave: a segment of consecutive paths per request, tables through pinned staging
-            pt::WfPlan plan;
-            std::vector<pt::WfSegment> segs;
-            std::vector<uint32_t> npix, spp, depth;
-            std::vector<pt::WfItem> witems;
-            uint64_t slot = 0;
-            for (size_t i = 0; i < wave_reqs.size(); ++i) {
-                Request* r = wave_reqs[i];
-                witems.push_back(pt::WfItem{(const pt::RenderParams*)r->dev, req_film(r), req_rgb(r), req_prim(r), r->npix, r->desc.spp});
-                npix.push_back(r->npix);
-                spp.push_back(r->desc.spp);
-                depth.push_back(r->desc.max_depth);
-                segs.push_back(pt::WfSegment{(uint32_t)i, 0, r->next_path, slot, wave_take[i]});
-                slot += wave_take[i];
-            }
-            pt::wf_add_wave(plan, segs, npix, spp, depth);
-            const size_t ib = up256(sizeof(pt::WfItem) * witems.size()), sb = up256(sizeof(pt::WfSegment) * plan.segments.size());
-            const size_t rb = up256(sizeof(pt::WfPixels) * plan.resolve.size());
-            std::memcpy(h_tables, witems.data(), sizeof(pt::WfItem) * witems.size());
-            std::memcpy(h_tables + ib, plan.segments.data(), sizeof(pt::WfSegment) * plan.segments.size());
-            std::memcpy(h_tables + ib + sb, plan.resolve.data(), sizeof(pt::WfPixels) * plan.resolve.size());
-            std::memcpy(h_tables + ib + sb + rb, plan.finish.data(), sizeof(pt::WfPixels) * plan.finish.size());
-            const size_t used = ib + sb + rb + sizeof(pt::WfPixels) * plan.finish.size();
-            if (e == cudaSuccess) e = cudaMemcpyAsync(d_tables, h_tables, used, cudaMemcpyHostToDevice, stream);
-            pt::WfTuning wt;
-            wt.threads_per_block = cfg.tuning.threads_per_block;
-            wt.queue_chunk = cfg.tuning.queue_chunk;
-            wt.stack_cap = cap;
-            char* dt = (char*)d_tables;
-            if (e == cudaSuccess)
-                e = pt::wf_launch_wave((const pt::WfItem*)dt, (const pt::WfSegment*)(dt + ib), (const pt::WfPixels*)(dt + ib + sb),
-                                       (const pt::WfPixels*)(dt + ib + sb + rb), plan.waves[0], ws, wt,
-                                       (unsigned long long*)d_counters + 1, stream);
+        if (stopping && queued.empty()) return;
+        const bool launched = !w.members.empty();
+        if (launched) {
+            w.slot = next_slot;
+            next_slot = (next_slot + 1) % kWavesQueued;
+            w.launch = enqueue(w, take, first);
+            queued.push_back(std::move(w));
         }
-        unsigned long long rays = 0;
-        if (e == cudaSuccess) e = cudaMemcpyAsync(&rays, (unsigned long long*)d_counters + 1, 8, cudaMemcpyDeviceToHost, stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-        const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
-        std::vector<Request*> finished;
-        {
-            std::lock_guard<std::mutex> lock(mu);
-            busy_ms += ms;
-            ++waves;
-            rays_traced += rays;
-            for (size_t i = 0; i < wave_reqs.size(); ++i) {
-                Request* r = wave_reqs[i];
-                if (e != cudaSuccess) {
-                    r->state = PT_ECUDA;
-                    worker_error = std::string("serving wave: ") + cudaGetErrorString(e);
-                } else if (wavefront) {
-                    r->next_path += wave_take[i];
-                } else {
-                    r->next_px += wave_take[i];
-                }
-                const bool complete = wavefront ? r->next_path == r->total_paths : r->next_px == r->npix;
-                if (r->state < 0 || complete) finished.push_back(r);
-            }
+        // Retire the oldest wave when the queue is full, or when there was nothing to launch
+        // (its completion frees memory and in-flight slots for the next admissions).
+        if (!queued.empty() && (queued.size() >= (size_t)kWavesQueued || !launched)) {
+            retire(queued.front());
+            queued.pop_front();
         }
-        for (Request* r : finished) {  // copy films out, release device memory
-            if (r->state == 1) {
-                r->rgb.resize(3 * (size_t)r->npix);
-                r->prim.resize(r->npix);
-                cudaError_t ce = cudaMemcpy(r->rgb.data(), req_rgb(r), 12 * (size_t)r->npix, cudaMemcpyDeviceToHost);
-                if (ce == cudaSuccess) ce = cudaMemcpy(r->prim.data(), req_prim(r), 4 * (size_t)r->npix, cudaMemcpyDeviceToHost);
-                r->state = ce == cudaSuccess ? 2 : PT_ECUDA;
-            }
-            cudaFree(r->dev);
-            r->dev = nullptr;
-            std::lock_guard<std::mutex> lock(mu);
-            r->done = Clock::now();
-            mem_in_use -= r->bytes;
-            active.erase(std::remove(active.begin(), active.end(), r), active.end());
-            ++completed;
-        }
-        if (!finished.empty()) done_cv.notify_all();
     }
 }
 
 using namespace pt;
 
+namespace {
+void destroy_resources(pt_server* s) {
+    for (int i = 0; i < kWavesQueued; ++i) {
+        if (s->ev_start[i]) cudaEventDestroy(s->ev_start[i]);
+        if (s->ev_end[i]) cudaEventDestroy(s->ev_end[i]);
+        if (s->ev_copied[i]) cudaEventDestroy(s->ev_copied[i]);
+    }
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->d_items) cudaFree(s->d_items);
+    if (s->d_counters) cudaFree(s->d_counters);
+    if (s->h_items) cudaFreeHost(s->h_items);
+    if (s->h_rays) cudaFreeHost(s->h_rays);
+    if (s->d_wave) cudaFree(s->d_wave);
+    if (s->d_tables) cudaFree(s->d_tables);
+    if (s->h_tables) cudaFreeHost(s->h_tables);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
+    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
+    for (auto& kv : s->all)
+        if (kv.second->host) s->pinned.put(kv.second->host, kv.second->host_bytes);
+    s->pinned.clear();
+    if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
+    if (s->stream) cudaStreamDestroy(s->stream);
+}
+}  // namespace
+
 extern "C" int pt_server_create(const pt_server_config* cfg, pt_server** out) {
     if (!cfg || !out) return fail(PT_EINVAL, "cfg or out is NULL");
     *out = nullptr;
     if (cfg->max_inflight == 0 || cfg->max_inflight > 65536) return fail(PT_EINVAL, "max_inflight must be in [1, 65536]");
+    if (cfg->policy != PT_SERVE_OLDEST_FIRST && cfg->policy != PT_SERVE_FAIR_SHARE) return fail(PT_EINVAL, "unknown policy");
     int rc = check_tuning(cfg->tuning);
     if (rc) return rc;
     std::unique_ptr<pt_server> s(new pt_server());
@@ -262,33 +435,42 @@ extern "C" int pt_server_create(const pt_server_config* cfg, pt_server** out) {
     if (!s->cfg.wave_pixels) s->cfg.wave_pixels = 1u << 20;
     if (cudaGetDevice(&s->device) != cudaSuccess) return fail(PT_ECUDA, "no CUDA device available");
     s->max_items = std::min<uint32_t>(cfg->max_inflight, 4096);
-    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMalloc(&s->d_items, sizeof(BatchItem) * s->max_items) != cudaSuccess ||
-        cudaMallocHost((void**)&s->h_items, sizeof(BatchItem) * s->max_items) != cudaSuccess ||
-        cudaMalloc(&s->d_counters, 16) != cudaSuccess) {
-        if (s->stream) cudaStreamDestroy(s->stream);
-        if (s->d_items) cudaFree(s->d_items);
-        if (s->h_items) cudaFreeHost(s->h_items);
-        return fail(PT_ENOMEM, "server buffers");
+    s->wavefront = cfg->tuning.pipeline != PT_PIPELINE_FUSED;
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = s->device;
+    bool ok = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&s->copy_stream, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaMemPoolCreate(&s->pool, &props) == cudaSuccess &&
+              cudaMalloc(&s->d_items, sizeof(BatchItem) * s->max_items) == cudaSuccess &&
+              cudaMallocHost((void**)&s->h_items, sizeof(BatchItem) * s->max_items * kWavesQueued) == cudaSuccess &&
+              cudaMallocHost((void**)&s->h_rays, sizeof(unsigned long long) * kWavesQueued) == cudaSuccess &&
+              cudaMalloc(&s->d_counters, 16) == cudaSuccess && cudaMemset(s->d_counters, 0, 16) == cudaSuccess;
+    for (int i = 0; ok && i < kWavesQueued; ++i)
+        ok = cudaEventCreate(&s->ev_start[i]) == cudaSuccess && cudaEventCreate(&s->ev_end[i]) == cudaSuccess &&
+             cudaEventCreateWithFlags(&s->ev_copied[i], cudaEventDisableTiming) == cudaSuccess;
+    if (ok) {
+        // keep freed request memory in the pool for the next admissions instead of returning it
+        // to the driver at every synchronisation
+        uint64_t keep = ~0ull;
+        cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
-    s->wavefront = cfg->tuning.pipeline == PT_PIPELINE_WAVEFRONT;
-    if (s->wavefront) {
+    if (ok && s->wavefront) {
         const uint64_t cap_paths = std::min<uint64_t>(s->cfg.wave_pixels, 1ull << 26);
         const uint32_t n = s->max_items;
-        s->table_bytes = up256(sizeof(WfItem) * n) + up256(sizeof(WfSegment) * n) + up256(sizeof(WfPixels) * 2 * n) +
-                         sizeof(WfPixels) * n;
-        if (cudaMalloc(&s->d_wave, wf_state_bytes((uint32_t)cap_paths)) != cudaSuccess ||
-            cudaMalloc(&s->d_tables, s->table_bytes) != cudaSuccess ||
-            cudaMallocHost((void**)&s->h_tables, s->table_bytes) != cudaSuccess) {
-            if (s->d_wave) cudaFree(s->d_wave);
-            if (s->d_tables) cudaFree(s->d_tables);
-            cudaFree(s->d_items);
-            cudaFree(s->d_counters);
-            cudaFreeHost(s->h_items);
-            cudaStreamDestroy(s->stream);
-            return fail(PT_ENOMEM, "server wave buffers");
-        }
-        wf_state_carve(s->d_wave, (uint32_t)cap_paths, s->ws);
+        s->table_bytes = up256(up256(sizeof(WfItem) * n) + up256(sizeof(WfSegment) * n) + up256(sizeof(WfPixels) * 2 * n) +
+                               sizeof(WfPixels) * n);
+        const bool paths = cfg->tuning.pipeline == PT_PIPELINE_PATHS;
+        ok = cudaMalloc(&s->d_wave, wf_state_bytes((uint32_t)cap_paths, paths)) == cudaSuccess &&
+             cudaMalloc(&s->d_tables, s->table_bytes) == cudaSuccess &&
+             cudaMallocHost((void**)&s->h_tables, s->table_bytes * kWavesQueued) == cudaSuccess;
+        if (ok) wf_state_carve(s->d_wave, (uint32_t)cap_paths, s->ws, paths);
+    }
+    if (!ok) {
+        cudaGetLastError();
+        destroy_resources(s.get());
+        return fail(PT_ENOMEM, "server buffers");
     }
     pt_server* raw = s.get();
     s->worker = std::thread([raw] { raw->run(); });
@@ -300,7 +482,8 @@ extern "C" int pt_server_submit(pt_server* s, pt_scene* scene, const pt_render_d
     if (!s || !ticket) return fail(PT_EINVAL, "server or ticket is NULL");
     int rc = check_render_desc(scene, desc);
     if (rc) return rc;
-    if (desc->flags & PT_RENDER_WAVEFRONT) return fail(PT_EINVAL, "served requests run the fused pipeline");
+    if (desc->flags & (PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT))
+        return fail(PT_EINVAL, "served requests take the server's pipeline (no PT_RENDER_WAVEFRONT / PT_RENDER_PERSISTENT)");
     if (scene->device != s->device) return fail(PT_EINVAL, "scene lives on another device");
     if (!stack_cap_for(scene->max_depth, s->cfg.tuning.stack_depth)) return fail(PT_ESTACK, "tree too deep");
     std::unique_ptr<Request> r(new Request());
@@ -308,7 +491,7 @@ extern "C" int pt_server_submit(pt_server* s, pt_scene* scene, const pt_render_d
     r->desc = *desc;
     r->params = render_params(scene, desc);
     r->npix = desc->width * desc->height;
-    r->total_paths = (uint64_t)r->npix * desc->spp;
+    r->total = s->wavefront ? (uint64_t)r->npix * desc->spp : r->npix;
     r->submitted = Clock::now();
     std::lock_guard<std::mutex> lock(s->mu);
     if (s->stop) return fail(PT_EINVAL, "server is shutting down");
@@ -353,12 +536,15 @@ extern "C" int pt_server_fetch(pt_server* s, uint64_t ticket, float* rgb_out, ui
     Request* r = it->second.get();
     if (r->state < 0) {
         const int st = r->state;
+        s->pinned.put(r->host, r->host_bytes);
         s->all.erase(it);
         return fail(st, "request failed: " + s->worker_error);
     }
     if (r->state != 2) return fail(PT_EINVAL, "request not finished");
-    if (rgb_out) std::memcpy(rgb_out, r->rgb.data(), r->rgb.size() * sizeof(float));
-    if (primary_out) std::memcpy(primary_out, r->prim.data(), r->prim.size() * sizeof(uint32_t));
+    const size_t n = r->npix;
+    if (rgb_out) std::memcpy(rgb_out, r->host, 12 * n);
+    if (primary_out) std::memcpy(primary_out, (const char*)r->host + 12 * n, 4 * n);
+    s->pinned.put(r->host, r->host_bytes);
     s->all.erase(it);
     return PT_OK;
 }
@@ -383,16 +569,10 @@ extern "C" int pt_server_destroy(pt_server* s) {
         s->stop = true;
     }
     s->cv.notify_all();
-    if (s->worker.joinable()) s->worker.join();
+    if (s->worker.joinable()) s->worker.join();  // the worker retires its queued waves first
     for (auto& kv : s->all)
-        if (kv.second->dev) cudaFree(kv.second->dev);
-    cudaFree(s->d_items);
-    cudaFree(s->d_counters);
-    cudaFreeHost(s->h_items);
-    if (s->d_wave) cudaFree(s->d_wave);
-    if (s->d_tables) cudaFree(s->d_tables);
-    if (s->h_tables) cudaFreeHost(s->h_tables);
-    cudaStreamDestroy(s->stream);
+        if (kv.second->dev) cudaFreeAsync(kv.second->dev, s->stream);
+    destroy_resources(s);
     delete s;
     return PT_OK;
 }

@@ -203,6 +203,118 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WfItem* __restrict_
     }
 }
 
+// Whole paths of several renders in one persistent launch.  Each lane runs one path at a time
+// (the fused loop of path.cuh, with the same device functions in the same order, so results are
+// bit-identical): its current ray, closest-hit or shadow, is walked leaf by leaf (walk_to_leaf /
+// walk_leaf, while-while), and when it ends the lane shades, starts the path's next ray, or
+// stores the clamped radiance and takes the next slot.  Warps take slots in chunks of `chunk`
+// from *fetch and refill idle lanes from the chunk, so a warp no longer waits for its longest
+// path.  The first SH stack entries of a lane live in shared memory.
+template <int CAP, int SH>
+__global__ void __launch_bounds__(128) wf_path_kernel(const WfItem* __restrict__ items, const WfSegment* __restrict__ segs,
+                                                      uint32_t nseg, uint32_t count, float* __restrict__ radiance,
+                                                      unsigned long long* fetch, uint32_t chunk,
+                                                      unsigned long long* rays_traced) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const float inf = bitsf(0x7F800000u);
+    __shared__ uint32_t sstack[SH > 0 ? SH * 128 : 1];
+    RayWalkT<CAP, SH> k;
+    k.stack.base = sstack + threadIdx.x;
+    k.stack.stride = 128;
+    uint64_t pool_next = 0, pool_end = 0;
+    bool exhausted = false, active = false, shadow = false, pending = false;
+    uint32_t slot = 0, pixel = 0, sample = 0, num_nodes = 0, rays = 0;
+    const RenderParams* p = nullptr;
+    uint32_t* primary = nullptr;
+    const uint4* nodes = nullptr;
+    const float4* tris = nullptr;
+    PathState s;
+    F3 contrib = f3(0.f, 0.f, 0.f);
+    while (true) {
+        const uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
+        if (need && !exhausted && pool_next >= pool_end) {
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(fetch, (unsigned long long)chunk);
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            if (base >= count) {
+                exhausted = true;
+            } else {
+                pool_next = base;
+                pool_end = base + chunk < count ? base + chunk : count;
+            }
+        }
+        if (need) {
+            const uint64_t avail = pool_end - pool_next;
+            const uint32_t rank = __popc(need & lt_mask);
+            if (!active && rank < avail) {
+                slot = (uint32_t)(pool_next + rank);
+                const WfSegment sg = segs[find_segment(segs, nseg, slot)];
+                const WfItem& it = items[sg.item];
+                p = it.params;
+                primary = it.primary;
+                nodes = (const uint4*)p->nodes;
+                tris = (const float4*)p->tris;
+                num_nodes = p->num_nodes;
+                path_camera(*p, sg.local_begin + (slot - sg.slot_base), pixel, sample, s.o, s.d);
+                s.src = f3(1.f, 1.f, 1.f);
+                s.L = f3(0.f, 0.f, 0.f);
+                s.bounces = 0;
+                s.last_lambert = 0;
+                shadow = false;
+                walk_begin(k, s.o.x, s.o.y, s.o.z, s.d.x, s.d.y, s.d.z, inf, false);
+                active = true;
+            }
+            const uint64_t took = (uint64_t)__popc(need) < avail ? (uint64_t)__popc(need) : avail;
+            pool_next += took;
+        }
+        if (!__any_sync(0xFFFFFFFFu, active)) {
+            if (exhausted) break;
+            continue;
+        }
+        if (active) {
+            uint32_t leaf_off = 0, leaf_n = 0;
+            const bool ok = walk_to_leaf<false>(k, nodes, num_nodes, leaf_off, leaf_n);
+            if (ok && leaf_n) walk_leaf<false>(k, tris, leaf_off, leaf_n);
+            if (!ok || k.done || k.sp == 0) {
+                ++rays;
+                bool go = false;
+                if (!ok) {
+                    raise_flag(p->err);
+                } else if (!shadow) {
+                    if (s.bounces == 0 && sample == 0 && primary) primary[pixel] = k.prim;
+                    ShadowReq sh;
+                    const bool more = shade_hit(*p, s, k.prim, k.leaf, k.u, k.v, k.w, pixel, sample, sh);
+                    if (sh.valid) {
+                        contrib = sh.contrib;
+                        pending = more;
+                        shadow = true;
+                        walk_begin(k, sh.o.x, sh.o.y, sh.o.z, sh.wi.x, sh.wi.y, sh.wi.z, sh.tmax, true);
+                    } else {
+                        go = more;
+                    }
+                } else {
+                    if (k.prim == kPrimNone) s.L = vadd(s.L, contrib);
+                    shadow = false;
+                    go = pending;
+                }
+                if (!shadow) {
+                    if (go && !throughput_is_zero(s.src)) {
+                        walk_begin(k, s.o.x, s.o.y, s.o.z, s.d.x, s.d.y, s.d.z, inf, false);
+                    } else {
+                        clamp_store(radiance + 3 * (size_t)slot, s.L);
+                        active = false;
+                    }
+                }
+            }
+        }
+    }
+    if (rays_traced) {
+        const uint32_t sum = __reduce_add_sync(0xFFFFFFFFu, rays);
+        if (lane == 0 && sum) atomicAdd(rays_traced, (unsigned long long)sum);
+    }
+}
+
 __global__ void wf_advance_kernel(uint32_t* counters, uint32_t consumed) {
     counters[consumed] = 0;
     counters[2] = 0;
@@ -255,36 +367,42 @@ __global__ void __launch_bounds__(256) wf_finish_kernel(const WfItem* __restrict
 
 // ---- host side --------------------------------------------------------------------------------
 
-size_t wf_state_bytes(uint32_t cap) {
+// The persistent path kernel (paths_only) needs only the radiance and the counters.
+size_t wf_state_bytes(uint32_t cap, bool paths_only) {
     size_t n = 0;
     auto take = [&](size_t b) { n += (b + 255) & ~(size_t)255; };
-    for (int k = 0; k < 4; ++k) take(16 * (size_t)cap);  // ray_o, ray_d, thr, rad
-    take(8 * (size_t)cap);                               // path
-    take(16 * (size_t)cap);                              // hit
-    take(4 * (size_t)cap);                               // hit_w
-    take(4 * (size_t)cap);
-    take(4 * (size_t)cap);                               // queues
-    for (int k = 0; k < 3; ++k) take(16 * (size_t)cap);  // shadow queue
-    take(12 * (size_t)cap);                              // radiance
-    take(64);                                            // counters
+    if (!paths_only) {
+        for (int k = 0; k < 4; ++k) take(16 * (size_t)cap);  // ray_o, ray_d, thr, rad
+        take(8 * (size_t)cap);                               // path
+        take(16 * (size_t)cap);                              // hit
+        take(4 * (size_t)cap);                               // hit_w
+        take(4 * (size_t)cap);
+        take(4 * (size_t)cap);                               // queues
+        for (int k = 0; k < 3; ++k) take(16 * (size_t)cap);  // shadow queue
+    }
+    take(12 * (size_t)cap);                                  // radiance
+    take(64);                                                // counters
     return n;
 }
 
-void wf_state_carve(void* base, uint32_t cap, WfState& ws) {
+void wf_state_carve(void* base, uint32_t cap, WfState& ws, bool paths_only) {
     char* q = (char*)base;
     auto take = [&](size_t b) { char* r = q; q += (b + 255) & ~(size_t)255; return r; };
-    ws.ray_o = (float4*)take(16 * (size_t)cap);
-    ws.ray_d = (float4*)take(16 * (size_t)cap);
-    ws.thr = (float4*)take(16 * (size_t)cap);
-    ws.rad = (float4*)take(16 * (size_t)cap);
-    ws.path = (uint64_t*)take(8 * (size_t)cap);
-    ws.hit = (uint4*)take(16 * (size_t)cap);
-    ws.hit_w = (float*)take(4 * (size_t)cap);
-    ws.queue[0] = (uint32_t*)take(4 * (size_t)cap);
-    ws.queue[1] = (uint32_t*)take(4 * (size_t)cap);
-    ws.sh_o = (float4*)take(16 * (size_t)cap);
-    ws.sh_d = (float4*)take(16 * (size_t)cap);
-    ws.sh_c = (float4*)take(16 * (size_t)cap);
+    ws = WfState{};
+    if (!paths_only) {
+        ws.ray_o = (float4*)take(16 * (size_t)cap);
+        ws.ray_d = (float4*)take(16 * (size_t)cap);
+        ws.thr = (float4*)take(16 * (size_t)cap);
+        ws.rad = (float4*)take(16 * (size_t)cap);
+        ws.path = (uint64_t*)take(8 * (size_t)cap);
+        ws.hit = (uint4*)take(16 * (size_t)cap);
+        ws.hit_w = (float*)take(4 * (size_t)cap);
+        ws.queue[0] = (uint32_t*)take(4 * (size_t)cap);
+        ws.queue[1] = (uint32_t*)take(4 * (size_t)cap);
+        ws.sh_o = (float4*)take(16 * (size_t)cap);
+        ws.sh_d = (float4*)take(16 * (size_t)cap);
+        ws.sh_c = (float4*)take(16 * (size_t)cap);
+    }
     ws.radiance = (float*)take(12 * (size_t)cap);
     ws.counters = (uint32_t*)take(64);
     ws.capacity = cap;
@@ -377,6 +495,35 @@ cudaError_t launch_trace_stage(const WfItem* items, const WfState& ws, const uin
     return cudaGetLastError();
 }
 
+template <int CAP>
+cudaError_t launch_path_stage(const WfItem* items, const WfSegment* segs, uint32_t nseg, uint32_t count, float* radiance,
+                              unsigned long long* fetch, uint32_t chunk, unsigned long long* rays, cudaStream_t s) {
+    constexpr int SH = 16;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wf_path_kernel<CAP, SH>, 128, 0);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    uint64_t grid = (uint64_t)sms * per_sm;
+    const uint64_t grid_needed = (((uint64_t)count + chunk - 1) / chunk * 32 + 127) / 128;
+    if (grid > grid_needed) grid = grid_needed ? grid_needed : 1;
+    e = cudaMemsetAsync(fetch, 0, sizeof(unsigned long long), s);
+    if (e != cudaSuccess) return e;
+    wf_path_kernel<CAP, SH><<<(unsigned)grid, 128, 0, s>>>(items, segs, nseg, count, radiance, fetch, chunk, rays);
+    return cudaGetLastError();
+}
+
+cudaError_t path_stage(int cap, const WfItem* items, const WfSegment* segs, uint32_t nseg, uint32_t count, float* radiance,
+                       unsigned long long* fetch, uint32_t chunk, unsigned long long* rays, cudaStream_t s) {
+    switch (cap) {
+        case 24: return launch_path_stage<24>(items, segs, nseg, count, radiance, fetch, chunk, rays, s);
+        case 32: return launch_path_stage<32>(items, segs, nseg, count, radiance, fetch, chunk, rays, s);
+        case 48: return launch_path_stage<48>(items, segs, nseg, count, radiance, fetch, chunk, rays, s);
+        default: return launch_path_stage<64>(items, segs, nseg, count, radiance, fetch, chunk, rays, s);
+    }
+}
+
 template <bool SHADOW>
 cudaError_t trace_stage(int cap, const WfItem* items, const WfState& ws, const uint32_t* queue, const uint32_t* count_ptr,
                         unsigned long long* fetch, const WfTuning& t, unsigned long long* rays, cudaStream_t s) {
@@ -387,13 +534,10 @@ cudaError_t trace_stage(int cap, const WfItem* items, const WfState& ws, const u
         default: return launch_trace_stage<64, SHADOW>(items, ws, queue, count_ptr, fetch, t, rays, s);
     }
 }
-}  // namespace
-
-cudaError_t wf_launch_wave(const WfItem* d_items, const WfSegment* d_segments, const WfPixels* d_resolve,
-                           const WfPixels* d_finish, const WfWave& w, const WfState& ws, const WfTuning& t,
-                           unsigned long long* rays_traced, cudaStream_t s) {
-    if (w.count == 0) return cudaSuccess;
-    if (w.count > ws.capacity) return cudaErrorInvalidValue;
+// Camera rays of the wave's slots, then per bounce: extend, shade (queue the next rays and the
+// shadow rays), shadow; finally the clamped radiance of every slot.
+cudaError_t bounce_stages(const WfItem* d_items, const WfSegment* d_segments, const WfWave& w, const WfState& ws,
+                          const WfTuning& t, unsigned long long* rays_traced, cudaStream_t s) {
     const uint32_t blocks = (w.count + 127) / 128;
     wf_init_kernel<<<blocks, 128, 0, s>>>(d_items, d_segments + w.seg_begin, w.seg_count, w.count, ws);
     cudaError_t e = cudaGetLastError();
@@ -415,6 +559,20 @@ cudaError_t wf_launch_wave(const WfItem* d_items, const WfSegment* d_segments, c
     }
     if (e != cudaSuccess) return e;
     wf_store_kernel<<<(w.count + 255) / 256, 256, 0, s>>>(ws, w.count);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t wf_launch_wave(const WfItem* d_items, const WfSegment* d_segments, const WfPixels* d_resolve,
+                           const WfPixels* d_finish, const WfWave& w, const WfState& ws, const WfTuning& t,
+                           unsigned long long* rays_traced, cudaStream_t s) {
+    if (w.count == 0) return cudaSuccess;
+    if (w.count > ws.capacity) return cudaErrorInvalidValue;
+    if (!t.paths && !ws.ray_o) return cudaErrorInvalidValue;  // state carved for the path kernel only
+    cudaError_t e = t.paths ? path_stage(t.stack_cap, d_items, d_segments + w.seg_begin, w.seg_count, w.count, ws.radiance,
+                                         (unsigned long long*)(ws.counters + 4), t.queue_chunk, rays_traced, s)
+                            : bounce_stages(d_items, d_segments, w, ws, t, rays_traced, s);
+    if (e != cudaSuccess) return e;
     if (w.res_pixels)
         wf_resolve_kernel<<<(unsigned)((w.res_pixels + 255) / 256), 256, 0, s>>>(d_items, d_segments, d_resolve + w.res_begin,
                                                                                  w.res_count, w.res_pixels, ws.radiance);

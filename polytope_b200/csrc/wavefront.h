@@ -65,13 +65,16 @@ struct WfState {
     uint32_t capacity;
 };
 
-size_t wf_state_bytes(uint32_t capacity);
-void wf_state_carve(void* base, uint32_t capacity, WfState& ws);
+// Device bytes of the state of `capacity` slots, and its layout in one buffer.  paths_only keeps
+// just the radiance and the counters (all the persistent path kernel uses).
+size_t wf_state_bytes(uint32_t capacity, bool paths_only = false);
+void wf_state_carve(void* base, uint32_t capacity, WfState& ws, bool paths_only = false);
 
 struct WfTuning {
     uint32_t threads_per_block = 128;  // extend / shadow kernels
     uint32_t queue_chunk = 64;         // rays a warp takes per fetch in the persistent kernels
     int stack_cap = 64;                // traversal stack entries
+    bool paths = false;                // one thread per whole path instead of per-bounce kernels
 };
 
 // One wave: `count` slots, `bounces` extend/shade/shadow iterations, and its ranges in the plan's
@@ -102,7 +105,7 @@ void wf_add_wave(WfPlan& plan, const std::vector<WfSegment>& segs, const std::ve
 void wf_plan_all(WfPlan& plan, const std::vector<uint32_t>& npix, const std::vector<uint32_t>& spp,
                  const std::vector<uint32_t>& max_depth, uint64_t wave_paths);
 
-// Enqueues one wave on `s`.  d_items / d_segments / d_resolve / d_finish are device copies of the
+// Enqueues one wave on `s` (per-bounce kernels, or with t.paths one kernel running whole paths).  d_items / d_segments / d_resolve / d_finish are device copies of the
 // plan's tables (the wave's ranges index into them).
 cudaError_t wf_launch_wave(const WfItem* d_items, const WfSegment* d_segments, const WfPixels* d_resolve,
                            const WfPixels* d_finish, const WfWave& w, const WfState& ws, const WfTuning& t,

@@ -30,7 +30,7 @@ def solo(scene, rd):
                           fov=rd.camera.fov_deg), rd.seed, rd.flags)
 
 
-@pytest.mark.parametrize("pipeline", [0, 1], ids=["fused", "wavefront"])
+@pytest.mark.parametrize("pipeline", [0, 1, 2], ids=["fused", "wavefront", "paths"])
 def test_batch_films_equal_solo_renders(cuda_device, pipeline):
     jobs = small_jobs()
     t = pb.default_tuning()
@@ -51,14 +51,15 @@ def test_batch_tunings_and_autotune(cuda_device):
     jobs = small_jobs(6, seed=9)
     ref = [solo(s, rd)[0] for s, rd in jobs]
     for tpb, chunk, stack, wave, pipe in ((64, 32, 0, 0, 0), (256, 128, 64, 1000, 0), (128, 64, 48, 3000, 0),
-                                          (128, 64, 0, 0, 1), (64, 32, 32, 700, 1), (256, 128, 64, 5000, 1)):
+                                          (128, 64, 0, 0, 1), (64, 32, 32, 700, 1), (256, 128, 64, 5000, 1),
+                                          (128, 64, 0, 0, 2), (64, 32, 24, 900, 2)):
         t = pb.BatchTuning(wave, tpb, stack, chunk, pipe)
         b = pb.Batch(jobs, t)
         b.run()
         for i in range(len(jobs)):
             assert_bit_equal(b.output(i)[0], ref[i], f"tuning {tpb}/{chunk}/{stack}/{wave} item {i}")
     best, ms, trials = pb.autotune(jobs)
-    assert ms > 0 and len(trials) >= 4
+    assert ms > 0 and len(trials) >= 5
     assert best.threads_per_block in (64, 128, 256) and best.queue_chunk % 32 == 0
     b = pb.Batch(jobs, best)
     b.run()
@@ -71,10 +72,11 @@ def tuning(pipeline):
     return t
 
 
-@pytest.mark.parametrize("pipeline", [0, 1], ids=["fused", "wavefront"])
-def test_server_results_same_alone_and_in_the_mix(cuda_device, pipeline):
+@pytest.mark.parametrize("policy", [pb.SERVE_OLDEST_FIRST, pb.SERVE_FAIR_SHARE], ids=["oldest", "fair"])
+@pytest.mark.parametrize("pipeline", [0, 1, 2], ids=["fused", "wavefront", "paths"])
+def test_server_results_same_alone_and_in_the_mix(cuda_device, pipeline, policy):
     jobs = small_jobs(12, seed=13)
-    srv = pb.Server(max_inflight=64, wave_pixels=2048, tuning=tuning(pipeline))
+    srv = pb.Server(max_inflight=64, wave_pixels=2048, tuning=tuning(pipeline), policy=policy)
     alone = []
     for scene, rd in jobs:  # one request at a time
         t = srv.submit(scene, rd)
@@ -94,7 +96,7 @@ def test_server_results_same_alone_and_in_the_mix(cuda_device, pipeline):
     srv.close()
 
 
-@pytest.mark.parametrize("pipeline", [0, 1], ids=["fused", "wavefront"])
+@pytest.mark.parametrize("pipeline", [0, 1, 2], ids=["fused", "wavefront", "paths"])
 def test_server_admission_by_memory_budget(cuda_device, pipeline):
     jobs = small_jobs(6, seed=17)
     # budget for about one request's film at a time: admissions wait for memory to free up

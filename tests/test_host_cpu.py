@@ -55,6 +55,13 @@ def test_invalid_arguments():
     empty = pb.Mesh([0.0], [0.0], [0.0], np.zeros((0, 3), np.uint32))
     with pytest.raises(pb.PolytopeError):
         pb.bvh_build([empty])
+    # server configuration is checked before any device call
+    cfg = pb.ServerConfig()
+    cfg.max_inflight, cfg.tuning, cfg.policy = 4, pb.default_tuning(), 7
+    h = C.c_void_p()
+    assert lib.pt_server_create(C.byref(cfg), C.byref(h)) == pb.PT_EINVAL and "policy" in pb.last_error()
+    cfg.policy, cfg.max_inflight = pb.SERVE_FAIR_SHARE, 0
+    assert lib.pt_server_create(C.byref(cfg), C.byref(h)) == pb.PT_EINVAL
 
 
 def soup(seed, meshes=3, faces=2000):

@@ -23,10 +23,10 @@ def image_errors(a, b):
     return rel, np.abs(a - b).mean() / max(np.abs(b).mean(), 1e-30)
 
 
-PIPELINES = [0, pb.RENDER_WAVEFRONT]
+PIPELINES = [0, pb.RENDER_WAVEFRONT, pb.RENDER_PERSISTENT]
 
 
-@pytest.mark.parametrize("pipeline", PIPELINES, ids=["fused", "wavefront"])
+@pytest.mark.parametrize("pipeline", PIPELINES, ids=["fused", "wavefront", "persistent"])
 def test_small_scene_render_matches_reference_fixture(cuda_device, pipeline):
     g = load_golden("small_scene.npz")
     meshes, env = W.small_scene()
@@ -39,7 +39,7 @@ def test_small_scene_render_matches_reference_fixture(cuda_device, pipeline):
         assert_bit_equal(prim, g[f"prim_{key}"], f"primary ids {key}")
 
 
-@pytest.mark.parametrize("pipeline", PIPELINES, ids=["fused", "wavefront"])
+@pytest.mark.parametrize("pipeline", PIPELINES, ids=["fused", "wavefront", "persistent"])
 def test_small_scene_full_config_matches_oracle(cuda_device, pipeline):
     """320x240, 8 spp, depth 4, NEE: the full small configuration against the CPU oracle."""
     meshes, env = W.small_scene()
@@ -54,7 +54,7 @@ def test_small_scene_full_config_matches_oracle(cuda_device, pipeline):
     assert rgb.mean() > 1.0
 
 
-@pytest.mark.parametrize("pipeline", PIPELINES, ids=["fused", "wavefront"])
+@pytest.mark.parametrize("pipeline", PIPELINES, ids=["fused", "wavefront", "persistent"])
 def test_instanced_scene_matches_reference_fixture(cuda_device, pipeline):
     g = load_golden("instanced_small.npz")
     im, env = W.instanced_scene(level=4)
@@ -65,7 +65,8 @@ def test_instanced_scene_matches_reference_fixture(cuda_device, pipeline):
 
 
 @pytest.mark.parametrize("flags", [pb.RENDER_JITTER | pb.RENDER_NEE, pb.RENDER_JITTER,
-                                   pb.RENDER_JITTER | pb.RENDER_NEE | pb.RENDER_WAVEFRONT])
+                                   pb.RENDER_JITTER | pb.RENDER_NEE | pb.RENDER_WAVEFRONT,
+                                   pb.RENDER_JITTER | pb.RENDER_NEE | pb.RENDER_PERSISTENT])
 def test_jitter_and_small_waves(cuda_device, flags):
     meshes, env = W.small_scene(level=3)
     scene = pb.Scene(meshes, env)
@@ -77,6 +78,14 @@ def test_jitter_and_small_waves(cuda_device, flags):
     orgb, oprim = po.OracleScene(meshes, env).render(dict(d, flags=flags))
     assert_bit_equal(rgb, orgb, "film")
     assert_bit_equal(prim, oprim, "prim")
+
+
+def test_pipeline_flags_exclude_each_other(cuda_device):
+    meshes, env = W.small_scene(level=1)
+    scene = pb.Scene(meshes, env)
+    with pytest.raises(pb.PolytopeError) as e:
+        pb.render(scene, 8, 8, 1, 2, W.SMALL_CAMERA, flags=pb.RENDER_WAVEFRONT | pb.RENDER_PERSISTENT)
+    assert e.value.code == pb.PT_EINVAL
 
 
 def test_runner_interface(cuda_device):
