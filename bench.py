@@ -298,6 +298,21 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
     return out
 
 
+def t_error_vs_f64(mesh, rays, hits, limit=1_000_000):
+    """Relative error of the FP32 t of closest hits against the FP64 ray-plane distance of the
+    same triangle (the microbench mesh has an identity transform, so its vertices are world space)."""
+    import polytope_b200 as pb
+    sel = np.nonzero((hits["prim"] != pb.PRIM_NONE) & (rays["flags"] == 0))[0][:limit]
+    vx = np.stack([mesh.x, mesh.y, mesh.z], 1).astype(np.float64)
+    f = np.asarray(mesh.faces)[hits["prim"][sel]]
+    v0, v1, v2 = vx[f[:, 0]], vx[f[:, 1]], vx[f[:, 2]]
+    org, d = rays["org"][sel].astype(np.float64), rays["dir"][sel].astype(np.float64)
+    nrm = np.cross(v1 - v0, v2 - v0)
+    t64 = ((v0 - org) * nrm).sum(1) / (d * nrm).sum(1)
+    rel = np.abs(hits["t"][sel] - t64) / np.abs(t64)
+    return {"closest_hits_checked": int(len(sel)), "max_rel": float(rel.max()), "mean_rel": float(rel.mean())}
+
+
 def make_workload(n_rays):
     from polytope_b200 import workloads as W
     return W.microbench(n_rays=n_rays)
@@ -383,6 +398,7 @@ def main():
     # counted pass (untimed): per-ray node / face tests for the algorithmic-bytes numerator
     hits_np, nt, tt = scene.intersect(rays, counts=True)
     alg_bytes = float(32 * nt.sum(dtype=np.uint64) + 44 * tt.sum(dtype=np.uint64) + (28 + 16) * n)
+    t_err = t_error_vs_f64(meshes[0], rays, hits_np)
 
     d_rays = torch.from_numpy(rays.view(np.uint8)).to(dev)
     d_hits = torch.zeros(n * 16, dtype=torch.uint8, device=dev)
@@ -460,6 +476,7 @@ def main():
                          "frac": round(achieved / peak, 4), "traffic": traffic,
                          "note": f"algorithmic bytes {alg_bytes / 1e9:.2f} GB per launch (reference node/face test counts); peak {peak_kind}"},
             "clocks": clk,
+            "t_error_vs_fp64": t_err,
             "step_ms": {"min": round(min(per), 4), "median": round(statistics.median(per), 4), "max": round(max(per), 4)},
         }
         if not args.no_batched and world == 1:

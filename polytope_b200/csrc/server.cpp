@@ -9,10 +9,10 @@
 // join the next wave and their work overlaps on the device.
 //
 // Two waves are kept queued on the stream: while the GPU runs wave k the host plans and enqueues
-// wave k+1, then retires wave k.  The films of the requests that finish in a wave are copied to
-// pinned host blocks on a second stream right behind the wave's kernels, so the copies overlap the
-// next wave; retiring waits for those copies and releases the requests' device memory, which is
-// stream-ordered, so no call here synchronises the whole device.  Pixels are independent and
+// wave k+1, then retires wave k (waits for its event) and hands the requests it finished to a
+// copier thread, which copies their films to host memory on a second stream while the next waves
+// run, then releases their device memory.  Request memory is stream-ordered (a pool owned by the
+// server), so no call here synchronises the whole device.  Pixels are independent and
 // each pixel's samples are summed in sample order, so a request's film is bit-identical whether
 // it ran alone or in any mix.
 
@@ -52,8 +52,8 @@ struct Request {
     void* dev = nullptr;          // RenderParams, rgb (3 floats/px), primary ids, film sums (wavefront)
     int state = 0;                // 0 queued, 1 admitted, 2 done, < 0 error
     Clock::time_point submitted, done;
-    void* host = nullptr;         // pinned block: rgb (3 floats/px) then primary ids, once finished
-    size_t host_bytes = 0;        // the block's size class
+    std::unique_ptr<float[]> rgb;      // host film (3 floats/px), once finished
+    std::unique_ptr<uint32_t[]> prim;  // host primary ids
 };
 
 static_assert(sizeof(pt::RenderParams) <= 256, "request layout reserves 256 bytes for the parameters");
@@ -65,49 +65,6 @@ size_t request_bytes(uint32_t npix, bool wavefront) {
 float* req_rgb(const Request* r) { return (float*)((char*)r->dev + 256); }
 uint32_t* req_prim(const Request* r) { return (uint32_t*)((char*)r->dev + 256 + up256(12 * (size_t)r->npix)); }
 float* req_film(const Request* r) { return (float*)((char*)r->dev + 256 + up256(12 * (size_t)r->npix) + up256(4 * (size_t)r->npix)); }
-
-// Pinned host blocks for finished films, cached by power-of-two size class: page-locking memory is
-// slow, and copies into pinned memory run at full link speed.
-class PinnedCache {
-  public:
-    void* get(size_t bytes, size_t& cls) {
-        cls = 1u << 16;
-        while (cls < bytes) cls <<= 1;
-        auto& v = free_[cls];
-        if (!v.empty()) {
-            void* p = v.back();
-            v.pop_back();
-            cached_ -= cls;
-            return p;
-        }
-        void* p = nullptr;
-        if (cudaMallocHost(&p, cls) != cudaSuccess) {
-            cudaGetLastError();
-            return nullptr;
-        }
-        return p;
-    }
-    void put(void* p, size_t cls) {
-        if (!p) return;
-        if (cached_ + cls > kMaxCached) {
-            cudaFreeHost(p);
-            return;
-        }
-        free_[cls].push_back(p);
-        cached_ += cls;
-    }
-    void clear() {
-        for (auto& kv : free_)
-            for (void* p : kv.second) cudaFreeHost(p);
-        free_.clear();
-        cached_ = 0;
-    }
-
-  private:
-    static constexpr size_t kMaxCached = 1ull << 30;
-    std::unordered_map<size_t, std::vector<void*>> free_;
-    size_t cached_ = 0;
-};
 
 // A wave enqueued on the stream and not yet retired.
 struct WaveInFlight {
@@ -126,6 +83,10 @@ struct pt_server {
     std::mutex mu;
     std::condition_variable cv;       // new work or stop
     std::condition_variable done_cv;  // a request finished
+    std::condition_variable copy_cv;  // finished requests to copy out, or stop
+    std::deque<Request*> to_copy;
+    bool stop_copier = false;
+    std::thread copier;
     std::deque<Request*> pending;
     std::vector<Request*> active;     // admission order
     std::unordered_map<uint64_t, std::unique_ptr<Request>> all;
@@ -137,8 +98,7 @@ struct pt_server {
     cudaStream_t stream = nullptr;       // waves
     cudaStream_t copy_stream = nullptr;  // film copies to host
     cudaMemPool_t pool = nullptr;        // request memory (stream-ordered)
-    cudaEvent_t ev_start[kWavesQueued] = {}, ev_end[kWavesQueued] = {}, ev_copied[kWavesQueued] = {};
-    PinnedCache pinned;                  // guarded by mu
+    cudaEvent_t ev_start[kWavesQueued] = {}, ev_end[kWavesQueued] = {};
     void* d_items = nullptr;
     pt::BatchItem* h_items = nullptr;    // pinned, kWavesQueued * max_items
     void* d_counters = nullptr;          // [0] fetch counter of the fused launch, [1] rays traced (cumulative)
@@ -156,6 +116,7 @@ struct pt_server {
     double busy_ms = 0.0;
 
     void run();
+    void copy_out();
     void admit();
     void plan(WaveInFlight& w, std::vector<uint32_t>& take, std::vector<uint64_t>& first);
     cudaError_t enqueue(WaveInFlight& w, const std::vector<uint32_t>& take, const std::vector<uint64_t>& first);
@@ -297,32 +258,14 @@ cudaError_t pt_server::enqueue(WaveInFlight& w, const std::vector<uint32_t>& tak
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_rays + w.slot, rays, 8, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaEventRecord(ev_end[w.slot], stream);
-    // films of the requests this wave finishes: device -> pinned, behind the wave's kernels
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(copy_stream, ev_end[w.slot], 0);
-    for (Request* r : w.finishing) {
-        if (e != cudaSuccess) break;
-        const size_t n = r->npix;
-        {
-            std::lock_guard<std::mutex> lock(mu);
-            r->host = pinned.get(16 * n, r->host_bytes);
-        }
-        if (!r->host) {
-            e = cudaErrorMemoryAllocation;
-            break;
-        }
-        e = cudaMemcpyAsync(r->host, req_rgb(r), 12 * n, cudaMemcpyDeviceToHost, copy_stream);
-        if (e == cudaSuccess)
-            e = cudaMemcpyAsync((char*)r->host + 12 * n, req_prim(r), 4 * n, cudaMemcpyDeviceToHost, copy_stream);
-    }
-    if (e == cudaSuccess) e = cudaEventRecord(ev_copied[w.slot], copy_stream);
     return e;
 }
 
-// Frees a request's device memory after everything queued so far on the stream and drops it
-// from the active set (mu held).
+// Frees a request's device memory (stream-ordered on the copy stream, after its film copies) and
+// drops it from the active set (mu held).
 void pt_server::release(Request* r) {
     if (r->dev) {
-        cudaFreeAsync(r->dev, stream);
+        cudaFreeAsync(r->dev, copy_stream);
         r->dev = nullptr;
         mem_in_use -= r->bytes;
     }
@@ -331,10 +274,10 @@ void pt_server::release(Request* r) {
     ++completed;
 }
 
-// Waits for a wave and for the copies of the films it finished, then releases those requests.
+// Waits for a wave; hands the requests it finished to the copier.
 void pt_server::retire(WaveInFlight& w) {
     cudaError_t e = w.launch;
-    if (e == cudaSuccess) e = cudaEventSynchronize(ev_copied[w.slot]);
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev_end[w.slot]);
     float ms = 0.f;
     if (e == cudaSuccess) cudaEventElapsedTime(&ms, ev_start[w.slot], ev_end[w.slot]);
     {
@@ -343,11 +286,8 @@ void pt_server::retire(WaveInFlight& w) {
         ++waves;
         if (e == cudaSuccess) {
             rays_traced = h_rays[w.slot];
-            for (Request* r : w.finishing) {
-                if (r->state != 1) continue;
-                r->state = 2;
-                release(r);
-            }
+            for (Request* r : w.finishing)
+                if (r->state == 1) to_copy.push_back(r);
         } else {
             worker_error = std::string("serving wave: ") + cudaGetErrorString(e);
             for (Request* r : w.members) {
@@ -356,7 +296,44 @@ void pt_server::retire(WaveInFlight& w) {
             }
         }
     }
+    copy_cv.notify_one();
     done_cv.notify_all();
+}
+
+// Copier thread: films of finished requests to host memory, then their device memory back to the
+// pool.  Runs beside the scheduler, so copies overlap the waves that follow.
+void pt_server::copy_out() {
+    cudaSetDevice(device);
+    while (true) {
+        Request* r = nullptr;
+        {
+            std::unique_lock<std::mutex> lock(mu);
+            copy_cv.wait(lock, [&] { return stop_copier || !to_copy.empty(); });
+            if (to_copy.empty()) return;  // stop_copier and nothing left
+            r = to_copy.front();
+            to_copy.pop_front();
+        }
+        const size_t n = r->npix;
+        std::unique_ptr<float[]> rgb(new (std::nothrow) float[3 * n]);
+        std::unique_ptr<uint32_t[]> prim(new (std::nothrow) uint32_t[n]);
+        cudaError_t e = rgb && prim ? cudaSuccess : cudaErrorMemoryAllocation;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(rgb.get(), req_rgb(r), 12 * n, cudaMemcpyDeviceToHost, copy_stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(prim.get(), req_prim(r), 4 * n, cudaMemcpyDeviceToHost, copy_stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(copy_stream);
+        {
+            std::lock_guard<std::mutex> lock(mu);
+            if (e == cudaSuccess) {
+                r->rgb = std::move(rgb);
+                r->prim = std::move(prim);
+                r->state = 2;
+            } else {
+                r->state = e == cudaErrorMemoryAllocation ? PT_ENOMEM : PT_ECUDA;
+                worker_error = std::string("copying a film out: ") + cudaGetErrorString(e);
+            }
+            release(r);
+        }
+        done_cv.notify_all();
+    }
 }
 
 void pt_server::run() {
@@ -403,7 +380,6 @@ void destroy_resources(pt_server* s) {
     for (int i = 0; i < kWavesQueued; ++i) {
         if (s->ev_start[i]) cudaEventDestroy(s->ev_start[i]);
         if (s->ev_end[i]) cudaEventDestroy(s->ev_end[i]);
-        if (s->ev_copied[i]) cudaEventDestroy(s->ev_copied[i]);
     }
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->d_items) cudaFree(s->d_items);
@@ -413,11 +389,8 @@ void destroy_resources(pt_server* s) {
     if (s->d_wave) cudaFree(s->d_wave);
     if (s->d_tables) cudaFree(s->d_tables);
     if (s->h_tables) cudaFreeHost(s->h_tables);
-    if (s->pool) cudaMemPoolDestroy(s->pool);
     if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
-    for (auto& kv : s->all)
-        if (kv.second->host) s->pinned.put(kv.second->host, kv.second->host_bytes);
-    s->pinned.clear();
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->stream) cudaStreamDestroy(s->stream);
 }
@@ -448,8 +421,7 @@ extern "C" int pt_server_create(const pt_server_config* cfg, pt_server** out) {
               cudaMallocHost((void**)&s->h_rays, sizeof(unsigned long long) * kWavesQueued) == cudaSuccess &&
               cudaMalloc(&s->d_counters, 16) == cudaSuccess && cudaMemset(s->d_counters, 0, 16) == cudaSuccess;
     for (int i = 0; ok && i < kWavesQueued; ++i)
-        ok = cudaEventCreate(&s->ev_start[i]) == cudaSuccess && cudaEventCreate(&s->ev_end[i]) == cudaSuccess &&
-             cudaEventCreateWithFlags(&s->ev_copied[i], cudaEventDisableTiming) == cudaSuccess;
+        ok = cudaEventCreate(&s->ev_start[i]) == cudaSuccess && cudaEventCreate(&s->ev_end[i]) == cudaSuccess;
     if (ok) {
         // keep freed request memory in the pool for the next admissions instead of returning it
         // to the driver at every synchronisation
@@ -474,6 +446,7 @@ extern "C" int pt_server_create(const pt_server_config* cfg, pt_server** out) {
     }
     pt_server* raw = s.get();
     s->worker = std::thread([raw] { raw->run(); });
+    s->copier = std::thread([raw] { raw->copy_out(); });
     *out = s.release();
     return PT_OK;
 }
@@ -536,15 +509,13 @@ extern "C" int pt_server_fetch(pt_server* s, uint64_t ticket, float* rgb_out, ui
     Request* r = it->second.get();
     if (r->state < 0) {
         const int st = r->state;
-        s->pinned.put(r->host, r->host_bytes);
         s->all.erase(it);
         return fail(st, "request failed: " + s->worker_error);
     }
     if (r->state != 2) return fail(PT_EINVAL, "request not finished");
     const size_t n = r->npix;
-    if (rgb_out) std::memcpy(rgb_out, r->host, 12 * n);
-    if (primary_out) std::memcpy(primary_out, (const char*)r->host + 12 * n, 4 * n);
-    s->pinned.put(r->host, r->host_bytes);
+    if (rgb_out) std::memcpy(rgb_out, r->rgb.get(), 12 * n);
+    if (primary_out) std::memcpy(primary_out, r->prim.get(), 4 * n);
     s->all.erase(it);
     return PT_OK;
 }
@@ -570,6 +541,12 @@ extern "C" int pt_server_destroy(pt_server* s) {
     }
     s->cv.notify_all();
     if (s->worker.joinable()) s->worker.join();  // the worker retires its queued waves first
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stop_copier = true;
+    }
+    s->copy_cv.notify_all();
+    if (s->copier.joinable()) s->copier.join();  // then the copier drains what they finished
     for (auto& kv : s->all)
         if (kv.second->dev) cudaFreeAsync(kv.second->dev, s->stream);
     destroy_resources(s);

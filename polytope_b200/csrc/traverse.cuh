@@ -29,32 +29,29 @@ constexpr int kStackCap = PT_TRAVERSAL_STACK;
 
 struct RayState {
     float ox, oy, oz;
-    float dx, dy, dz;
     float ix, iy, iz;          // 1/d (bvh.cpp:477-481)
-    int kx, ky, kz;            // Wald axis permutation (mesh.cpp:196-211)
+    int kz;                    // Wald axis permutation (mesh.cpp:196-211): kx = kz+1, ky = kx+1 (mod 3)
     float sx, sy, sz;          // shear constants (mesh.cpp:234-236)
-    float okx, oky, okz;       // permuted origin
-    float dkx, dky, dkz;
 };
 
 PT_HD float sel3(int k, float x, float y, float z) { return k == 0 ? x : (k == 1 ? y : z); }
+PT_HD int next_axis(int k) { return k == 2 ? 0 : k + 1; }
 
+// Only what the box and face tests read is kept, so a ray costs few registers in the persistent
+// kernels; the permuted direction is needed only here, for the shear constants.
 PT_HD void ray_setup(RayState& r, float ox, float oy, float oz, float dx, float dy, float dz) {
     r.ox = ox; r.oy = oy; r.oz = oz;
-    r.dx = dx; r.dy = dy; r.dz = dz;
     r.ix = frcp(dx); r.iy = frcp(dy); r.iz = frcp(dz);
     const float ax = fabs_(dx), ay = fabs_(dy), az = fabs_(dz);
     int kz = 0;
     if (ay > ax && ay > az) kz = 1;
     else if (az > ax && az > ay) kz = 2;
-    int kx = kz + 1; if (kx == 3) kx = 0;
-    int ky = kx + 1; if (ky == 3) ky = 0;
-    r.kx = kx; r.ky = ky; r.kz = kz;
-    r.dkx = sel3(kx, dx, dy, dz); r.dky = sel3(ky, dx, dy, dz); r.dkz = sel3(kz, dx, dy, dz);
-    r.okx = sel3(kx, ox, oy, oz); r.oky = sel3(ky, ox, oy, oz); r.okz = sel3(kz, ox, oy, oz);
-    r.sx = fdiv(-r.dkx, r.dkz);
-    r.sy = fdiv(-r.dky, r.dkz);
-    r.sz = frcp(r.dkz);
+    const int kx = next_axis(kz), ky = next_axis(kx);
+    r.kz = kz;
+    const float dkx = sel3(kx, dx, dy, dz), dky = sel3(ky, dx, dy, dz), dkz = sel3(kz, dx, dy, dz);
+    r.sx = fdiv(-dkx, dkz);
+    r.sy = fdiv(-dky, dkz);
+    r.sz = frcp(dkz);
 }
 
 // BoundingBox::Hits with the running MinT as the far bound.
@@ -101,13 +98,15 @@ PT_HD float max3abs(float x, float y, float z) {  // max_component(abs(v)), mesh
 PT_HD bool wald(const RayState& r, float v0x, float v0y, float v0z, float v1x, float v1y,
                                      float v1z, float v2x, float v2y, float v2z, float min_t, float& t_out,
                                      float& u_out, float& v_out, float& w_out) {
-    // p_it = permute(v_i - O)
-    float p0x = fsub(sel3(r.kx, v0x, v0y, v0z), r.okx), p0y = fsub(sel3(r.ky, v0x, v0y, v0z), r.oky),
-          p0z = fsub(sel3(r.kz, v0x, v0y, v0z), r.okz);
-    float p1x = fsub(sel3(r.kx, v1x, v1y, v1z), r.okx), p1y = fsub(sel3(r.ky, v1x, v1y, v1z), r.oky),
-          p1z = fsub(sel3(r.kz, v1x, v1y, v1z), r.okz);
-    float p2x = fsub(sel3(r.kx, v2x, v2y, v2z), r.okx), p2y = fsub(sel3(r.ky, v2x, v2y, v2z), r.oky),
-          p2z = fsub(sel3(r.kz, v2x, v2y, v2z), r.okz);
+    // p_it = permute(v_i - O): per-component differences, then the axis permutation (a select of
+    // exact differences, so the same values as permuting first)
+    const int kz = r.kz, kx = next_axis(kz), ky = next_axis(kx);
+    const float a0x = fsub(v0x, r.ox), a0y = fsub(v0y, r.oy), a0z = fsub(v0z, r.oz);
+    const float a1x = fsub(v1x, r.ox), a1y = fsub(v1y, r.oy), a1z = fsub(v1z, r.oz);
+    const float a2x = fsub(v2x, r.ox), a2y = fsub(v2y, r.oy), a2z = fsub(v2z, r.oz);
+    float p0x = sel3(kx, a0x, a0y, a0z), p0y = sel3(ky, a0x, a0y, a0z), p0z = sel3(kz, a0x, a0y, a0z);
+    float p1x = sel3(kx, a1x, a1y, a1z), p1y = sel3(ky, a1x, a1y, a1z), p1z = sel3(kz, a1x, a1y, a1z);
+    float p2x = sel3(kx, a2x, a2y, a2z), p2y = sel3(ky, a2x, a2y, a2z), p2z = sel3(kz, a2x, a2y, a2z);
     p0x = ffma(r.sx, p0z, p0x); p0y = ffma(r.sy, p0z, p0y);
     p1x = ffma(r.sx, p1z, p1x); p1y = ffma(r.sy, p1z, p1y);
     p2x = ffma(r.sx, p2z, p2x); p2y = ffma(r.sy, p2z, p2y);

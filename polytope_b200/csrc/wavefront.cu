@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WfItem* __restrict_
 // from *fetch and refill idle lanes from the chunk, so a warp no longer waits for its longest
 // path.  The first SH stack entries of a lane live in shared memory.
 template <int CAP, int SH>
-__global__ void __launch_bounds__(128) wf_path_kernel(const WfItem* __restrict__ items, const WfSegment* __restrict__ segs,
+__global__ void __launch_bounds__(128, 5) wf_path_kernel(const WfItem* __restrict__ items, const WfSegment* __restrict__ segs,
                                                       uint32_t nseg, uint32_t count, float* __restrict__ radiance,
                                                       unsigned long long* fetch, uint32_t chunk,
                                                       unsigned long long* rays_traced) {
