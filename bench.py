@@ -234,25 +234,38 @@ def serve_tuning(pb):
     return t
 
 
-def run_served(pb, scenes, reqs, arrivals, wave=1 << 23, policy=0, tuning=None):
-    """Submits each request at its arrival time; returns (latencies ms, makespan s, rays)."""
-    srv = pb.Server(max_inflight=64, wave_pixels=wave, tuning=tuning or serve_tuning(pb), policy=policy)
+def make_server(pb, wave=1 << 23, policy=0, tuning=None):
+    return pb.Server(max_inflight=64, wave_pixels=wave, tuning=tuning or serve_tuning(pb), policy=policy,
+                     host_budget=2 << 30)
+
+
+def run_served(pb, srv, scenes, reqs, arrivals):
+    """Submits each request at its arrival time while a client thread waits for and fetches the
+    results in submission order; returns (latencies ms, makespan s, rays)."""
+    import queue
+    import threading
+    rays0 = srv.stats()["rays_traced"]
+    lats = np.zeros(len(reqs))
+    q = queue.Queue()
+
+    def client():
+        for k in range(len(reqs)):
+            t = q.get()
+            srv.wait(t, 600000)
+            lats[k] = srv.poll(t)[1]
+            srv.fetch(t)
+
+    th = threading.Thread(target=client)
+    th.start()
     t0 = time.perf_counter()
-    tickets = []
     for (si, rd), at in zip(reqs, arrivals):
         now = time.perf_counter() - t0
         if at > now:
             time.sleep(at - now)
-        tickets.append(srv.submit(scenes[si], rd))
-    lats = []
-    for t in tickets:
-        srv.wait(t, 600000)
-        lats.append(srv.poll(t)[1])
-        srv.fetch(t)
+        q.put(srv.submit(scenes[si], rd))
+    th.join()
     span = time.perf_counter() - t0
-    rays = srv.stats()["rays_traced"]
-    srv.close()
-    return np.array(lats), span, rays
+    return lats, span, srv.stats()["rays_traced"] - rays0
 
 
 def run_plain(pb, scenes, reqs, arrivals):
@@ -275,18 +288,21 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
     from polytope_b200 import workloads as W
     scenes = build_scenes(pb, W.serving_pool(n_scenes))
     reqs, unit = serve_requests(pb, n_scenes, n_requests, seed)
-    warm = reqs[:8]
-    run_served(pb, scenes, warm, np.zeros(len(warm)))
-    run_plain(pb, scenes, warm, np.zeros(len(warm)))
+    # one long-running service for every rate; both arms are warmed on the whole request list
+    # (memory pools, host arena, lazily loaded kernels), submitted at once
+    srv = make_server(pb)
+    run_served(pb, srv, scenes, reqs, np.zeros(len(reqs)))
+    run_plain(pb, scenes, reqs, np.zeros(len(reqs)))
     pct = lambda a, q: round(float(np.percentile(a, q)), 2)
     out = {"workload": f"{n_scenes} resident scenes (instanced displaced spheres, 100k-4M tris), {n_requests} Poisson requests per rate, "
                        "128^2-1024^2, 1/4/16 spp, depth 5, NEE",
-           "server": "path-wave pipeline, oldest-first waves of 8,388,608 paths, 2 waves queued",
+           "server": "one server for every rate: path-wave pipeline, oldest-first waves of 8,388,608 paths, 2 waves queued, "
+                     "films by DMA into a 2 GiB pinned arena; a client thread fetches results in submission order",
            "timing": "host steady clock from the first arrival to the last completion; latency = completion - arrival",
            "rates": []}
     for rate in rates:
         arrivals = unit / rate
-        lat_s, span_s, rays = run_served(pb, scenes, reqs, arrivals)
+        lat_s, span_s, rays = run_served(pb, srv, scenes, reqs, arrivals)
         lat_p, span_p = run_plain(pb, scenes, reqs, arrivals)
         out["rays"] = int(rays)
         out["rates"].append({
@@ -295,6 +311,7 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
                        "p99_ms": pct(lat_s, 99), "makespan_s": round(span_s, 3)},
             "plain_per_request": {"mrays_s": round(rays / span_p / 1e6, 1), "p50_ms": pct(lat_p, 50), "p95_ms": pct(lat_p, 95),
                                   "p99_ms": pct(lat_p, 99), "makespan_s": round(span_p, 3)}})
+    srv.close()
     return out
 
 

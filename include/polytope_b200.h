@@ -300,6 +300,8 @@ typedef struct pt_server_config {
     uint64_t        wave_pixels;      /* work per wave: pixels (PT_PIPELINE_FUSED) or paths (others) */
     pt_batch_tuning tuning;
     uint32_t        policy;           /* PT_SERVE_OLDEST_FIRST or PT_SERVE_FAIR_SHARE              */
+    uint64_t        host_budget;      /* pinned host bytes for finished films not yet fetched
+                                         (0 = 1 GiB); admission waits while it is full           */
 } pt_server_config;
 
 typedef struct pt_server_stats {
@@ -321,6 +323,13 @@ int pt_server_submit(pt_server *server, pt_scene *scene, const pt_render_desc *d
 /* latency_ms: submit to completion (-1 until done). */
 int pt_server_poll(pt_server *server, uint64_t ticket, int *state, double *latency_ms);
 int pt_server_wait(pt_server *server, uint64_t ticket, uint32_t timeout_ms, int *state);
+/* Where a request's latency went, in ms after submission (-1 for a stage not reached yet):
+ * admitted (device and host memory taken), first wave enqueued, last wave's kernels done on the
+ * GPU, film in host memory (the completion that pt_server_poll's latency reports). */
+typedef struct pt_request_timing {
+    double admitted_ms, first_wave_ms, last_wave_ms, done_ms;
+} pt_request_timing;
+int pt_server_timing(pt_server *server, uint64_t ticket, pt_request_timing *timing);
 /* Copies a finished request's film (width*height*3 floats) and primary ids, then forgets it. */
 int pt_server_fetch(pt_server *server, uint64_t ticket, float *rgb_out, uint32_t *primary_out);
 int pt_server_get_stats(pt_server *server, pt_server_stats *stats);

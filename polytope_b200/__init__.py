@@ -110,7 +110,12 @@ class BatchTuneResult(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("max_inflight", C.c_uint32), ("memory_budget", C.c_uint64), ("wave_pixels", C.c_uint64),
-                ("tuning", BatchTuning), ("policy", C.c_uint32)]
+                ("tuning", BatchTuning), ("policy", C.c_uint32), ("host_budget", C.c_uint64)]
+
+
+class RequestTiming(C.Structure):
+    _fields_ = [("admitted_ms", C.c_double), ("first_wave_ms", C.c_double), ("last_wave_ms", C.c_double),
+                ("done_ms", C.c_double)]
 
 
 class ServerStats(C.Structure):
@@ -148,6 +153,7 @@ def _load() -> C.CDLL:
         "pt_server_create": (i, [C.POINTER(ServerConfig), C.POINTER(_vp)]),
         "pt_server_submit": (i, [_vp, _vp, C.POINTER(RenderDesc), C.POINTER(u64)]),
         "pt_server_poll": (i, [_vp, u64, C.POINTER(i), C.POINTER(C.c_double)]),
+        "pt_server_timing": (i, [_vp, u64, C.POINTER(RequestTiming)]),
         "pt_server_wait": (i, [_vp, u64, u32, C.POINTER(i)]),
         "pt_server_fetch": (i, [_vp, u64, _vp, _vp]),
         "pt_server_get_stats": (i, [_vp, C.POINTER(ServerStats)]),
@@ -483,13 +489,14 @@ class Server:
     """Continuous batching of render requests over resident scenes (pt_server_*)."""
 
     def __init__(self, max_inflight: int = 64, memory_budget: int = 0, wave_pixels: int = 1 << 20,
-                 tuning: Optional[BatchTuning] = None, policy: int = 0):
+                 tuning: Optional[BatchTuning] = None, policy: int = 0, host_budget: int = 0):
         cfg = ServerConfig()
         cfg.max_inflight = max_inflight
         cfg.memory_budget = memory_budget
         cfg.wave_pixels = wave_pixels
         cfg.tuning = tuning if tuning is not None else default_tuning()
         cfg.policy = policy
+        cfg.host_budget = host_budget
         h = _vp()
         check(lib.pt_server_create(C.byref(cfg), C.byref(h)))
         self.handle = h
@@ -505,6 +512,11 @@ class Server:
         st, lat = C.c_int(0), C.c_double(0)
         check(lib.pt_server_poll(self.handle, ticket, C.byref(st), C.byref(lat)))
         return st.value, lat.value
+
+    def timing(self, ticket: int) -> dict:
+        t = RequestTiming()
+        check(lib.pt_server_timing(self.handle, ticket, C.byref(t)))
+        return {k: float(getattr(t, k)) for k, _ in t._fields_}
 
     def wait(self, ticket: int, timeout_ms: int = 60000) -> int:
         st = C.c_int(0)

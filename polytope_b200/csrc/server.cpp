@@ -1,26 +1,29 @@
 // server.cpp -- the serving loop: continuous batching of render requests over resident scenes.
 //
 // Scenes stay resident in HBM (pt_scene handles).  Requests (scene, resolution, spp, depth) are
-// queued by pt_server_submit; a scheduler thread admits them while the in-flight limit and the
-// device-memory budget (film + primary ids of each admitted request) allow, and plans waves: a
-// wave takes work (paths for the wavefront pipeline, pixels for the fused one) from the admitted
-// requests, oldest first (PT_SERVE_OLDEST_FIRST) or a fair share from each (PT_SERVE_FAIR_SHARE),
-// and traces it in one multi-render launch sequence, so requests that arrive while others run
-// join the next wave and their work overlaps on the device.
+// queued by pt_server_submit; a scheduler thread admits them while the in-flight limit, the
+// device-memory budget (parameters, film, primary ids and film sums of each request) and the
+// pinned host arena for finished films allow, and plans waves: a wave takes work (paths for the
+// wave pipelines, pixels for the fused one) from the admitted requests, oldest first
+// (PT_SERVE_OLDEST_FIRST) or a fair share from each (PT_SERVE_FAIR_SHARE), and traces it in one
+// multi-render launch sequence, so requests that arrive while others run join the next wave and
+// their work overlaps on the device.
 //
 // Two waves are kept queued on the stream: while the GPU runs wave k the host plans and enqueues
-// wave k+1, then retires wave k (waits for its event) and hands the requests it finished to a
-// copier thread, which copies their films to host memory on a second stream while the next waves
-// run, then releases their device memory.  Request memory is stream-ordered (a pool owned by the
-// server), so no call here synchronises the whole device.  Pixels are independent and
-// each pixel's samples are summed in sample order, so a request's film is bit-identical whether
-// it ran alone or in any mix.
+// wave k+1, then retires wave k.  The films of the requests a wave finishes are copied by DMA into
+// the pinned host arena on a second stream right behind the wave's kernels, so the copies overlap
+// the next wave and no host thread copies or page-faults on the completion path; retiring waits
+// for those copies and returns the requests' device memory to a stream-ordered pool owned by the
+// server, so no call here synchronises the whole device.  pt_server_fetch copies a film out of the
+// arena and frees its space.  Pixels are independent and each pixel's samples are summed in sample
+// order, so a request's film is bit-identical whether it ran alone or in any mix.
 
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <deque>
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -46,25 +49,64 @@ struct Request {
     pt_render_desc desc{};
     pt::RenderParams params{};
     uint32_t npix = 0;
-    uint64_t total = 0;           // work units: pixels (fused) or paths (wavefront, sample-major)
+    uint64_t total = 0;           // work units: pixels (fused) or paths (wave pipelines, sample-major)
     uint64_t planned = 0;         // units handed to waves so far
-    size_t bytes = 0;
-    void* dev = nullptr;          // RenderParams, rgb (3 floats/px), primary ids, film sums (wavefront)
+    size_t bytes = 0;             // device bytes
+    void* dev = nullptr;          // RenderParams, rgb (3 floats/px), primary ids, film sums (wave pipelines)
+    size_t host_off = ~(size_t)0; // finished film in the host arena: rgb then primary ids
     int state = 0;                // 0 queued, 1 admitted, 2 done, < 0 error
-    Clock::time_point submitted, done;
-    std::unique_ptr<float[]> rgb;      // host film (3 floats/px), once finished
-    std::unique_ptr<uint32_t[]> prim;  // host primary ids
+    bool launched = false, retired = false;
+    Clock::time_point submitted, admitted, first_wave, last_wave, done;
 };
 
 static_assert(sizeof(pt::RenderParams) <= 256, "request layout reserves 256 bytes for the parameters");
 
 size_t up256(size_t x) { return (x + 255) & ~(size_t)255; }
-size_t request_bytes(uint32_t npix, bool wavefront) {
-    return 256 + up256(12 * (size_t)npix) + up256(4 * (size_t)npix) + (wavefront ? 12 * (size_t)npix : 0);
+size_t request_bytes(uint32_t npix, bool wave_engine) {
+    return 256 + up256(12 * (size_t)npix) + up256(4 * (size_t)npix) + (wave_engine ? 12 * (size_t)npix : 0);
 }
+size_t host_bytes(uint32_t npix) { return up256(16 * (size_t)npix); }
 float* req_rgb(const Request* r) { return (float*)((char*)r->dev + 256); }
 uint32_t* req_prim(const Request* r) { return (uint32_t*)((char*)r->dev + 256 + up256(12 * (size_t)r->npix)); }
 float* req_film(const Request* r) { return (float*)((char*)r->dev + 256 + up256(12 * (size_t)r->npix) + up256(4 * (size_t)r->npix)); }
+
+// First-fit allocator over the pinned host arena (offsets; adjacent free blocks merge).
+class ArenaAllocator {
+  public:
+    void reset(size_t size) {
+        free_.clear();
+        if (size) free_[0] = size;
+    }
+    bool alloc(size_t n, size_t& off) {
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < n) continue;
+            off = it->first;
+            const size_t left = it->second - n;
+            free_.erase(it);
+            if (left) free_[off + n] = left;
+            return true;
+        }
+        return false;
+    }
+    void release(size_t off, size_t n) {
+        auto next = free_.lower_bound(off);
+        if (next != free_.end() && off + n == next->first) {
+            n += next->second;
+            next = free_.erase(next);
+        }
+        if (next != free_.begin()) {
+            auto prev = std::prev(next);
+            if (prev->first + prev->second == off) {
+                prev->second += n;
+                return;
+            }
+        }
+        free_[off] = n;
+    }
+
+  private:
+    std::map<size_t, size_t> free_;
+};
 
 // A wave enqueued on the stream and not yet retired.
 struct WaveInFlight {
@@ -81,31 +123,31 @@ struct pt_server {
     int device = 0;
     std::thread worker;
     std::mutex mu;
-    std::condition_variable cv;       // new work or stop
+    std::condition_variable cv;       // new work, freed memory, or stop
     std::condition_variable done_cv;  // a request finished
-    std::condition_variable copy_cv;  // finished requests to copy out, or stop
-    std::deque<Request*> to_copy;
-    bool stop_copier = false;
-    std::thread copier;
     std::deque<Request*> pending;
     std::vector<Request*> active;     // admission order
     std::unordered_map<uint64_t, std::unique_ptr<Request>> all;
     bool stop = false;
+    bool blocked = false;             // admission waits for device or host memory to free up
     uint64_t next_ticket = 1;
     size_t mem_in_use = 0;
     std::string worker_error;
     // device / pinned resources of the scheduler
     cudaStream_t stream = nullptr;       // waves
-    cudaStream_t copy_stream = nullptr;  // film copies to host
+    cudaStream_t copy_stream = nullptr;  // finished films -> host arena
     cudaMemPool_t pool = nullptr;        // request memory (stream-ordered)
-    cudaEvent_t ev_start[kWavesQueued] = {}, ev_end[kWavesQueued] = {};
+    cudaEvent_t ev_start[kWavesQueued] = {}, ev_end[kWavesQueued] = {}, ev_copied[kWavesQueued] = {};
+    char* arena = nullptr;               // pinned host memory for finished films
+    size_t arena_size = 0;
+    ArenaAllocator arena_alloc;          // guarded by mu
     void* d_items = nullptr;
     pt::BatchItem* h_items = nullptr;    // pinned, kWavesQueued * max_items
     void* d_counters = nullptr;          // [0] fetch counter of the fused launch, [1] rays traced (cumulative)
     unsigned long long* h_rays = nullptr;  // pinned, one per slot
     uint32_t max_items = 0;
-    // wavefront pipeline: wave state and per-wave tables (device + pinned staging per slot)
-    bool wavefront = false;              // work in paths through the wave engine (PT_PIPELINE_WAVEFRONT / _PATHS)
+    // wave pipelines: wave state and per-wave tables (device + pinned staging per slot)
+    bool wave_engine = false;            // PT_PIPELINE_WAVEFRONT or PT_PIPELINE_PATHS: work in paths
     void* d_wave = nullptr;
     pt::WfState ws{};
     void* d_tables = nullptr;
@@ -116,12 +158,11 @@ struct pt_server {
     double busy_ms = 0.0;
 
     void run();
-    void copy_out();
     void admit();
     void plan(WaveInFlight& w, std::vector<uint32_t>& take, std::vector<uint64_t>& first);
     cudaError_t enqueue(WaveInFlight& w, const std::vector<uint32_t>& take, const std::vector<uint64_t>& first);
     void retire(WaveInFlight& w);
-    void release(Request* r);  // with mu held
+    void release_device(Request* r);  // with mu held
     bool has_unplanned() const {
         for (const Request* r : active)
             if (r->state == 1 && r->planned < r->total) return true;
@@ -129,9 +170,9 @@ struct pt_server {
     }
 };
 
-// Admits queued requests in arrival order while the in-flight limit and the memory budget allow
-// (mu held).  With an empty active set one request is always tried, so a request larger than the
-// budget still runs alone.
+// Admits queued requests in arrival order while the in-flight limit, the device-memory budget and
+// the host arena allow (mu held).  With nothing admitted, one request is always tried against the
+// device, so a request larger than the budget still runs alone.
 void pt_server::admit() {
     if (pending.empty()) return;
     size_t budget = cfg.memory_budget;
@@ -143,25 +184,40 @@ void pt_server::admit() {
         cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
         budget = (size_t)(0.8 * (double)(free_b + (reserved > used ? reserved - used : 0))) + mem_in_use;
     }
+    blocked = false;
     while (!pending.empty() && active.size() < cfg.max_inflight) {
         Request* r = pending.front();
-        const size_t need = request_bytes(r->npix, wavefront);
-        if (mem_in_use + need > budget && !active.empty()) break;
+        const size_t need = request_bytes(r->npix, wave_engine);
+        if (mem_in_use + need > budget && !active.empty()) {
+            blocked = true;
+            break;
+        }
+        size_t off = 0;
+        if (!arena_alloc.alloc(host_bytes(r->npix), off)) {
+            blocked = true;  // finished films not fetched yet hold the arena
+            break;
+        }
         if (cudaMallocFromPoolAsync(&r->dev, need, pool, stream) != cudaSuccess) {
             cudaGetLastError();
             r->dev = nullptr;
-            if (!active.empty()) break;  // wait for memory to free up
+            arena_alloc.release(off, host_bytes(r->npix));
+            if (!active.empty()) {
+                blocked = true;
+                break;
+            }
             r->state = PT_ENOMEM;
             pending.pop_front();
             done_cv.notify_all();
             continue;
         }
+        r->host_off = off;
         r->bytes = need;
         mem_in_use += need;
         r->params.rays_traced = nullptr;
         cudaMemcpyAsync(r->dev, &r->params, sizeof(r->params), cudaMemcpyHostToDevice, stream);
-        if (wavefront) cudaMemsetAsync(req_film(r), 0, 12 * (size_t)r->npix, stream);
+        if (wave_engine) cudaMemsetAsync(req_film(r), 0, 12 * (size_t)r->npix, stream);
         r->state = 1;
+        r->admitted = Clock::now();
         pending.pop_front();
         active.push_back(r);
     }
@@ -170,7 +226,7 @@ void pt_server::admit() {
 // Picks the next wave's work (mu held): oldest admitted request first, each taking what it has
 // left up to the wave's room, or an equal share of the wave for every request.
 void pt_server::plan(WaveInFlight& w, std::vector<uint32_t>& take, std::vector<uint64_t>& first) {
-    uint64_t room = wavefront ? std::min<uint64_t>(cfg.wave_pixels, ws.capacity) : cfg.wave_pixels;
+    uint64_t room = wave_engine ? std::min<uint64_t>(cfg.wave_pixels, ws.capacity) : cfg.wave_pixels;
     uint64_t share = room;
     if (cfg.policy == PT_SERVE_FAIR_SHARE) {
         size_t open = 0;
@@ -182,6 +238,10 @@ void pt_server::plan(WaveInFlight& w, std::vector<uint32_t>& take, std::vector<u
         if (r->state != 1 || r->planned >= r->total) continue;
         const uint64_t t = std::min<uint64_t>(std::min<uint64_t>(share, r->total - r->planned), room);
         room -= t;
+        if (!r->launched) {
+            r->launched = true;
+            r->first_wave = Clock::now();
+        }
         w.members.push_back(r);
         take.push_back((uint32_t)t);
         first.push_back(r->planned);
@@ -190,15 +250,16 @@ void pt_server::plan(WaveInFlight& w, std::vector<uint32_t>& take, std::vector<u
     }
 }
 
-// Enqueues the wave's tables and kernels on the stream, then the rays-traced read-back and the
-// wave's end event.
+// Enqueues the wave's tables and kernels on the stream, the rays-traced read-back and the wave's
+// end event; then, on the copy stream behind that event, the DMA of every film the wave finishes
+// into the host arena, and the wave's copied event.
 cudaError_t pt_server::enqueue(WaveInFlight& w, const std::vector<uint32_t>& take, const std::vector<uint64_t>& first) {
     uint32_t max_depth = 0;
     for (Request* r : w.members) max_depth = std::max(max_depth, r->scene->max_depth);
     const int cap = pt::stack_cap_for(max_depth, cfg.tuning.stack_depth);
     unsigned long long* rays = (unsigned long long*)d_counters + 1;
     cudaError_t e = cudaEventRecord(ev_start[w.slot], stream);
-    if (!wavefront) {
+    if (!wave_engine) {
         pt::BatchItem* hi = h_items + (size_t)w.slot * max_items;
         uint64_t base = 0;
         for (size_t i = 0; i < w.members.size(); ++i) {
@@ -258,12 +319,21 @@ cudaError_t pt_server::enqueue(WaveInFlight& w, const std::vector<uint32_t>& tak
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(h_rays + w.slot, rays, 8, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaEventRecord(ev_end[w.slot], stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(copy_stream, ev_end[w.slot], 0);
+    for (Request* r : w.finishing) {
+        if (e != cudaSuccess) break;
+        char* h = arena + r->host_off;
+        const size_t n = r->npix;
+        e = cudaMemcpyAsync(h, req_rgb(r), 12 * n, cudaMemcpyDeviceToHost, copy_stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h + 12 * n, req_prim(r), 4 * n, cudaMemcpyDeviceToHost, copy_stream);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ev_copied[w.slot], copy_stream);
     return e;
 }
 
-// Frees a request's device memory (stream-ordered on the copy stream, after its film copies) and
-// drops it from the active set (mu held).
-void pt_server::release(Request* r) {
+// Returns a request's device memory to the pool, stream-ordered after its film copies, and drops
+// it from the active set (mu held).  Its film stays in the host arena until fetched.
+void pt_server::release_device(Request* r) {
     if (r->dev) {
         cudaFreeAsync(r->dev, copy_stream);
         r->dev = nullptr;
@@ -272,12 +342,15 @@ void pt_server::release(Request* r) {
     r->done = Clock::now();
     active.erase(std::remove(active.begin(), active.end(), r), active.end());
     ++completed;
+    blocked = false;
 }
 
-// Waits for a wave; hands the requests it finished to the copier.
+// Waits for a wave and the copies of the films it finished; those requests are done.
 void pt_server::retire(WaveInFlight& w) {
     cudaError_t e = w.launch;
     if (e == cudaSuccess) e = cudaEventSynchronize(ev_end[w.slot]);
+    const auto kernels_done = Clock::now();
+    if (e == cudaSuccess) e = cudaEventSynchronize(ev_copied[w.slot]);
     float ms = 0.f;
     if (e == cudaSuccess) cudaEventElapsedTime(&ms, ev_start[w.slot], ev_end[w.slot]);
     {
@@ -286,54 +359,22 @@ void pt_server::retire(WaveInFlight& w) {
         ++waves;
         if (e == cudaSuccess) {
             rays_traced = h_rays[w.slot];
-            for (Request* r : w.finishing)
-                if (r->state == 1) to_copy.push_back(r);
+            for (Request* r : w.finishing) {
+                r->retired = true;
+                r->last_wave = kernels_done;
+                if (r->state != 1) continue;
+                r->state = 2;
+                release_device(r);
+            }
         } else {
             worker_error = std::string("serving wave: ") + cudaGetErrorString(e);
             for (Request* r : w.members) {
                 if (r->state == 1) r->state = PT_ECUDA;
-                if (r->dev || std::find(active.begin(), active.end(), r) != active.end()) release(r);
+                if (r->dev || std::find(active.begin(), active.end(), r) != active.end()) release_device(r);
             }
         }
     }
-    copy_cv.notify_one();
     done_cv.notify_all();
-}
-
-// Copier thread: films of finished requests to host memory, then their device memory back to the
-// pool.  Runs beside the scheduler, so copies overlap the waves that follow.
-void pt_server::copy_out() {
-    cudaSetDevice(device);
-    while (true) {
-        Request* r = nullptr;
-        {
-            std::unique_lock<std::mutex> lock(mu);
-            copy_cv.wait(lock, [&] { return stop_copier || !to_copy.empty(); });
-            if (to_copy.empty()) return;  // stop_copier and nothing left
-            r = to_copy.front();
-            to_copy.pop_front();
-        }
-        const size_t n = r->npix;
-        std::unique_ptr<float[]> rgb(new (std::nothrow) float[3 * n]);
-        std::unique_ptr<uint32_t[]> prim(new (std::nothrow) uint32_t[n]);
-        cudaError_t e = rgb && prim ? cudaSuccess : cudaErrorMemoryAllocation;
-        if (e == cudaSuccess) e = cudaMemcpyAsync(rgb.get(), req_rgb(r), 12 * n, cudaMemcpyDeviceToHost, copy_stream);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(prim.get(), req_prim(r), 4 * n, cudaMemcpyDeviceToHost, copy_stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(copy_stream);
-        {
-            std::lock_guard<std::mutex> lock(mu);
-            if (e == cudaSuccess) {
-                r->rgb = std::move(rgb);
-                r->prim = std::move(prim);
-                r->state = 2;
-            } else {
-                r->state = e == cudaErrorMemoryAllocation ? PT_ENOMEM : PT_ECUDA;
-                worker_error = std::string("copying a film out: ") + cudaGetErrorString(e);
-            }
-            release(r);
-        }
-        done_cv.notify_all();
-    }
 }
 
 void pt_server::run() {
@@ -349,7 +390,8 @@ void pt_server::run() {
         bool stopping;
         {
             std::unique_lock<std::mutex> lock(mu);
-            if (queued.empty()) cv.wait(lock, [&] { return stop || !pending.empty() || has_unplanned(); });
+            if (queued.empty())
+                cv.wait(lock, [&] { return stop || (!pending.empty() && !blocked) || has_unplanned(); });
             stopping = stop;
             if (!stopping) {
                 admit();
@@ -377,19 +419,21 @@ using namespace pt;
 
 namespace {
 void destroy_resources(pt_server* s) {
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
     for (int i = 0; i < kWavesQueued; ++i) {
         if (s->ev_start[i]) cudaEventDestroy(s->ev_start[i]);
         if (s->ev_end[i]) cudaEventDestroy(s->ev_end[i]);
+        if (s->ev_copied[i]) cudaEventDestroy(s->ev_copied[i]);
     }
-    if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->d_items) cudaFree(s->d_items);
     if (s->d_counters) cudaFree(s->d_counters);
     if (s->h_items) cudaFreeHost(s->h_items);
     if (s->h_rays) cudaFreeHost(s->h_rays);
+    if (s->arena) cudaFreeHost(s->arena);
     if (s->d_wave) cudaFree(s->d_wave);
     if (s->d_tables) cudaFree(s->d_tables);
     if (s->h_tables) cudaFreeHost(s->h_tables);
-    if (s->copy_stream) cudaStreamSynchronize(s->copy_stream);
     if (s->pool) cudaMemPoolDestroy(s->pool);
     if (s->copy_stream) cudaStreamDestroy(s->copy_stream);
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -406,9 +450,10 @@ extern "C" int pt_server_create(const pt_server_config* cfg, pt_server** out) {
     std::unique_ptr<pt_server> s(new pt_server());
     s->cfg = *cfg;
     if (!s->cfg.wave_pixels) s->cfg.wave_pixels = 1u << 20;
+    s->arena_size = cfg->host_budget ? (size_t)up256(cfg->host_budget) : ((size_t)1 << 30);
     if (cudaGetDevice(&s->device) != cudaSuccess) return fail(PT_ECUDA, "no CUDA device available");
     s->max_items = std::min<uint32_t>(cfg->max_inflight, 4096);
-    s->wavefront = cfg->tuning.pipeline != PT_PIPELINE_FUSED;
+    s->wave_engine = cfg->tuning.pipeline != PT_PIPELINE_FUSED;
     cudaMemPoolProps props{};
     props.allocType = cudaMemAllocationTypePinned;
     props.location.type = cudaMemLocationTypeDevice;
@@ -419,16 +464,19 @@ extern "C" int pt_server_create(const pt_server_config* cfg, pt_server** out) {
               cudaMalloc(&s->d_items, sizeof(BatchItem) * s->max_items) == cudaSuccess &&
               cudaMallocHost((void**)&s->h_items, sizeof(BatchItem) * s->max_items * kWavesQueued) == cudaSuccess &&
               cudaMallocHost((void**)&s->h_rays, sizeof(unsigned long long) * kWavesQueued) == cudaSuccess &&
+              cudaMallocHost((void**)&s->arena, s->arena_size) == cudaSuccess &&
               cudaMalloc(&s->d_counters, 16) == cudaSuccess && cudaMemset(s->d_counters, 0, 16) == cudaSuccess;
     for (int i = 0; ok && i < kWavesQueued; ++i)
-        ok = cudaEventCreate(&s->ev_start[i]) == cudaSuccess && cudaEventCreate(&s->ev_end[i]) == cudaSuccess;
+        ok = cudaEventCreate(&s->ev_start[i]) == cudaSuccess && cudaEventCreate(&s->ev_end[i]) == cudaSuccess &&
+             cudaEventCreateWithFlags(&s->ev_copied[i], cudaEventDisableTiming) == cudaSuccess;
     if (ok) {
+        s->arena_alloc.reset(s->arena_size);
         // keep freed request memory in the pool for the next admissions instead of returning it
         // to the driver at every synchronisation
         uint64_t keep = ~0ull;
         cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
-    if (ok && s->wavefront) {
+    if (ok && s->wave_engine) {
         const uint64_t cap_paths = std::min<uint64_t>(s->cfg.wave_pixels, 1ull << 26);
         const uint32_t n = s->max_items;
         s->table_bytes = up256(up256(sizeof(WfItem) * n) + up256(sizeof(WfSegment) * n) + up256(sizeof(WfPixels) * 2 * n) +
@@ -446,7 +494,6 @@ extern "C" int pt_server_create(const pt_server_config* cfg, pt_server** out) {
     }
     pt_server* raw = s.get();
     s->worker = std::thread([raw] { raw->run(); });
-    s->copier = std::thread([raw] { raw->copy_out(); });
     *out = s.release();
     return PT_OK;
 }
@@ -464,7 +511,8 @@ extern "C" int pt_server_submit(pt_server* s, pt_scene* scene, const pt_render_d
     r->desc = *desc;
     r->params = render_params(scene, desc);
     r->npix = desc->width * desc->height;
-    r->total = s->wavefront ? (uint64_t)r->npix * desc->spp : r->npix;
+    if (host_bytes(r->npix) > s->arena_size) return fail(PT_EINVAL, "film larger than the server's host budget");
+    r->total = s->wave_engine ? (uint64_t)r->npix * desc->spp : r->npix;
     r->submitted = Clock::now();
     std::lock_guard<std::mutex> lock(s->mu);
     if (s->stop) return fail(PT_EINVAL, "server is shutting down");
@@ -489,6 +537,22 @@ extern "C" int pt_server_poll(pt_server* s, uint64_t ticket, int* state, double*
     return PT_OK;
 }
 
+extern "C" int pt_server_timing(pt_server* s, uint64_t ticket, pt_request_timing* t) {
+    if (!s || !t) return fail(PT_EINVAL, "server or timing is NULL");
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->all.find(ticket);
+    if (it == s->all.end()) return fail(PT_EINVAL, "unknown ticket");
+    const Request* r = it->second.get();
+    auto ms = [&](bool reached, Clock::time_point p) {
+        return reached ? std::chrono::duration<double, std::milli>(p - r->submitted).count() : -1.0;
+    };
+    t->admitted_ms = ms(r->state != 0, r->admitted);
+    t->first_wave_ms = ms(r->launched, r->first_wave);
+    t->last_wave_ms = ms(r->retired, r->last_wave);
+    t->done_ms = ms(r->state == 2, r->done);
+    return PT_OK;
+}
+
 extern "C" int pt_server_wait(pt_server* s, uint64_t ticket, uint32_t timeout_ms, int* state) {
     if (!s || !state) return fail(PT_EINVAL, "server or state is NULL");
     std::unique_lock<std::mutex> lock(s->mu);
@@ -507,16 +571,23 @@ extern "C" int pt_server_fetch(pt_server* s, uint64_t ticket, float* rgb_out, ui
     auto it = s->all.find(ticket);
     if (it == s->all.end()) return fail(PT_EINVAL, "unknown ticket");
     Request* r = it->second.get();
-    if (r->state < 0) {
-        const int st = r->state;
-        s->all.erase(it);
-        return fail(st, "request failed: " + s->worker_error);
-    }
-    if (r->state != 2) return fail(PT_EINVAL, "request not finished");
+    if (r->state != 2 && r->state >= 0) return fail(PT_EINVAL, "request not finished");
+    const int st = r->state;
     const size_t n = r->npix;
-    if (rgb_out) std::memcpy(rgb_out, r->rgb.get(), 12 * n);
-    if (primary_out) std::memcpy(primary_out, r->prim.get(), 4 * n);
+    if (st == 2) {
+        const char* h = s->arena + r->host_off;
+        if (rgb_out) std::memcpy(rgb_out, h, 12 * n);
+        if (primary_out) std::memcpy(primary_out, h + 12 * n, 4 * n);
+    }
+    if (r->host_off != ~(size_t)0) {
+        s->arena_alloc.release(r->host_off, host_bytes(r->npix));
+        s->blocked = false;
+    }
     s->all.erase(it);
+    const std::string err = s->worker_error;
+    lock.unlock();
+    s->cv.notify_one();  // admission may have waited for arena space
+    if (st < 0) return fail(st, "request failed: " + err);
     return PT_OK;
 }
 
@@ -541,12 +612,6 @@ extern "C" int pt_server_destroy(pt_server* s) {
     }
     s->cv.notify_all();
     if (s->worker.joinable()) s->worker.join();  // the worker retires its queued waves first
-    {
-        std::lock_guard<std::mutex> lock(s->mu);
-        s->stop_copier = true;
-    }
-    s->copy_cv.notify_all();
-    if (s->copier.joinable()) s->copier.join();  // then the copier drains what they finished
     for (auto& kv : s->all)
         if (kv.second->dev) cudaFreeAsync(kv.second->dev, s->stream);
     destroy_resources(s);

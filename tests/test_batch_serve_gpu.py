@@ -87,6 +87,9 @@ def test_server_results_same_alone_and_in_the_mix(cuda_device, pipeline, policy)
         assert srv.wait(t, 60000) == 2
         st, lat = srv.poll(t)
         assert st == 2 and lat >= 0
+        tm = srv.timing(t)
+        assert 0 <= tm["admitted_ms"] <= tm["first_wave_ms"] <= tm["last_wave_ms"] <= tm["done_ms"]
+        assert abs(tm["done_ms"] - lat) < 1e-6
         rgb, prim = srv.fetch(t)
         assert_bit_equal(rgb, a_rgb, "mix vs alone")
         assert_bit_equal(prim, a_prim, "mix vs alone prim")
@@ -105,6 +108,24 @@ def test_server_admission_by_memory_budget(cuda_device, pipeline):
     for t, (scene, rd) in zip(tickets, jobs):
         assert srv.wait(t, 60000) == 2
         assert_bit_equal(srv.fetch(t)[0], solo(scene, rd)[0], "budgeted")
+    srv.close()
+
+
+def test_server_host_budget_backpressure(cuda_device):
+    jobs = small_jobs(6, seed=29)
+    biggest = max(rd.width * rd.height for _, rd in jobs)
+    # room for about two finished films: later admissions wait until earlier results are fetched
+    srv = pb.Server(max_inflight=8, wave_pixels=4096, host_budget=2 * 16 * biggest + 512, tuning=tuning(pb.PIPELINE_PATHS))
+    tickets = [srv.submit(scene, rd) for scene, rd in jobs]
+    for t, (scene, rd) in zip(tickets, jobs):
+        assert srv.wait(t, 60000) == 2
+        assert_bit_equal(srv.fetch(t)[0], solo(scene, rd)[0], "host budget")
+    scene, rd = jobs[0]
+    small = pb.Server(max_inflight=2, host_budget=256)
+    with pytest.raises(pb.PolytopeError) as e:
+        small.submit(scene, rd)
+    assert e.value.code == pb.PT_EINVAL and "host budget" in str(e.value)
+    small.close()
     srv.close()
 
 
