@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(128) trace_kernel(const uint4* __restrict__ no
 // leaf's faces with the other lanes of the warp.  A ray's own node and face order is exactly the
 // reference's; only which rays share a warp changes.
 template <bool COUNT, int SH>
-__global__ void __launch_bounds__(128, 8) trace_persistent_kernel(const uint4* __restrict__ nodes,
+__global__ void __launch_bounds__(128, 9) trace_persistent_kernel(const uint4* __restrict__ nodes,
                                                                const float4* __restrict__ tris, uint32_t num_nodes,
                                                                const float4* __restrict__ rays, uint4* __restrict__ hits,
                                                                uint64_t n, uint32_t* node_tests, uint32_t* tri_tests,
