@@ -386,6 +386,9 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-render", action="store_true")
+    ap.add_argument("--render-probe", action="store_true",
+                    help="render the instanced scene at 480x270, 16 spp once with the plain launch and once with "
+                         "the persistent path kernel, then exit (a small case for profilers)")
     ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
 
@@ -394,6 +397,16 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.render_probe:
+        import polytope_b200 as pb
+        from polytope_b200 import workloads as W
+        meshes, env = W.instanced_scene()
+        scene = pb.Scene(meshes, env)
+        d = W.INSTANCED_RENDER
+        for fl in (0, pb.RENDER_PERSISTENT):
+            rgb, _ = pb.render(scene, 480, 270, 16, d["max_depth"], d["camera"], d["seed"], pb.RENDER_NEE | fl)
+            print(json.dumps({"render_probe": "480x270x16", "flags": pb.RENDER_NEE | fl, "mean": float(rgb.mean())}))
         return
 
     import torch
