@@ -315,6 +315,16 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
     return out
 
 
+def max_over_ranks(values, dist, device):
+    """Each value's maximum over all ranks (the slowest rank's time); unchanged on one rank."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t]
+
+
 def t_error_vs_f64(mesh, rays, hits, limit=1_000_000):
     """Relative error of the FP32 t of closest hits against the FP64 ray-plane distance of the
     same triangle (the microbench mesh has an identity transform, so its vertices are world space)."""
@@ -466,6 +476,8 @@ def main():
     h_hits = torch.zeros(n * 16, dtype=torch.uint8).pin_memory()
     for _ in range(2):
         pb.check(pb.lib.pt_trace(scene.handle, h_rays.data_ptr(), n, h_hits.data_ptr(), 0, None))
+    if dist:
+        dist.barrier()
     e2e_steps = max(3, min(args.steps, 10))
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -479,11 +491,7 @@ def main():
     assert h_hits.numpy().tobytes() == hits_np.tobytes(), "e2e hits differ"
     clk = clocks_summary(sampler)
 
-    ms = total_ms / args.steps
-    if dist:
-        t = torch.tensor([ms, e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, e2e_ms = float(t[0]), float(t[1])
+    ms, e2e_ms = max_over_ranks([total_ms / args.steps, e2e_ms], dist, dev)
     if rank == 0:
         value = n * world / (ms * 1e-3) / 1e6
         e2e = n * world / (e2e_ms * 1e-3) / 1e6
