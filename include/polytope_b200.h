@@ -234,6 +234,24 @@ int pt_render(pt_scene *scene, const pt_render_desc *desc, float *rgb_out,
 int pt_render_noalloc(pt_scene *scene, const pt_render_desc *desc, float *rgb_dev,
                       uint32_t *primary_dev, void *stream);
 
+/* ---- output format ------------------------------------------------------------------------ */
+
+/* The film as the reference's PNG output stores it: RGBA8, row-major, each channel
+ * (unsigned char)(v > 255 ? 255 : v) (truncation), alpha 255 -- PNGFilm::Output
+ * (src/cpu/films/PNGFilm.cpp:20-45) and OutputPNG::Output (src/cuda/png_output.cpp:29-36).
+ * Replaces the float-film download with 4 bytes per pixel.  rgb: width*height*3 floats on the
+ * device (a film from pt_render / pt_batch_output with PT_MEM_DEVICE); rgba_out: width*height*4
+ * bytes, host (the call returns when they are there) or device with PT_MEM_DEVICE (asynchronous
+ * on `stream`).  Films are non-negative; the reference's cast is undefined for negative or NaN
+ * values, which map to 0 here. */
+int pt_film_to_rgba8(const float *rgb_dev, uint32_t width, uint32_t height, uint8_t *rgba_out,
+                     uint32_t mem_flags, void *stream);
+
+/* Writes RGBA8 pixels (host memory) as a PNG file (8-bit RGBA, no interlace, zlib stream of
+ * stored blocks).  The decoded pixels equal what lodepng::encode writes for the same data in the
+ * reference (PNGFilm.cpp:50); the compressed bytes differ. */
+int pt_write_png(const char *path, const uint8_t *rgba, uint32_t width, uint32_t height);
+
 /* ---- batched renders (many uneven scenes in one persistent, graph-captured launch) -------- */
 
 /* One render of a batch.  The batch keeps its own device films; read them with pt_batch_output. */

@@ -1033,6 +1033,17 @@ int orc_wald(const float* tri9, const float* o, const float* d, float min_t, flo
     tuvw[0] = c.t; tuvw[1] = c.u; tuvw[2] = c.v; tuvw[3] = c.w;
     return 1;
 }
+// PNGFilm::Output (src/cpu/films/PNGFilm.cpp:27-44): RGBA8, each channel
+// static_cast<unsigned char>(v > 255 ? 255 : v), alpha 255, index 4 * (y * width + x).
+void orc_film_to_rgba8(const float* rgb, uint32_t npix, uint8_t* out) {
+    for (uint32_t i = 0; i < npix; ++i) {
+        const float r = rgb[3 * (size_t)i], g = rgb[3 * (size_t)i + 1], b = rgb[3 * (size_t)i + 2];
+        out[4 * (size_t)i + 0] = static_cast<unsigned char>(r > 255 ? 255 : r);
+        out[4 * (size_t)i + 1] = static_cast<unsigned char>(g > 255 ? 255 : g);
+        out[4 * (size_t)i + 2] = static_cast<unsigned char>(b > 255 ? 255 : b);
+        out[4 * (size_t)i + 3] = static_cast<unsigned char>(255);
+    }
+}
 float orc_gamma(int n) {
     switch (n) { case 2: return kGamma2; case 3: return kGamma3; case 5: return kGamma5; case 7: return kGamma7; default: return kGammaMul; }
 }

@@ -131,6 +131,7 @@ def oracle_lib() -> C.CDLL:
         lib.orc_world_to_local.argtypes = [_fp, _fp, _fp, _fp, _fp]
         lib.orc_mirror_sample.argtypes = [_fp, _fp]
         lib.orc_normalize.argtypes = [_fp]
+        lib.orc_film_to_rgba8.argtypes = [_fp, C.c_uint32, C.c_void_p]
         _oracle_lib = lib
     return _oracle_lib
 
@@ -312,3 +313,12 @@ def normalize(v):
     a = np.array(v, np.float32)
     oracle_lib().orc_normalize(_f(a))
     return a
+
+
+def film_to_rgba8(rgb: np.ndarray) -> np.ndarray:
+    """The film as PNGFilm::Output stores it (oracle restatement): (H, W, 4) uint8."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    h, w = rgb.shape[:2]
+    out = np.zeros((h, w, 4), np.uint8)
+    oracle_lib().orc_film_to_rgba8(_f(rgb), h * w, out.ctypes.data)
+    return out

@@ -143,6 +143,8 @@ def _load() -> C.CDLL:
         "pt_scene_get_trace_tuning": (i, [_vp, C.POINTER(TraceTuning)]),
         "pt_trace_autotune": (i, [_vp, _vp, u64, _vp, C.POINTER(TraceTuning), C.POINTER(C.c_float)]),
         "pt_render_noalloc": (i, [_vp, C.POINTER(RenderDesc), _vp, _vp, _vp]),
+        "pt_film_to_rgba8": (i, [_vp, u32, u32, _vp, u32, _vp]),
+        "pt_write_png": (i, [C.c_char_p, _vp, u32, u32]),
         "pt_batch_default_tuning": (i, [C.POINTER(BatchTuning)]),
         "pt_batch_create": (i, [C.POINTER(BatchItem), u32, C.POINTER(BatchTuning), C.POINTER(_vp)]),
         "pt_batch_run": (i, [_vp, _vp]),
@@ -363,6 +365,20 @@ def render(scene: Scene, width: int, height: int, spp: int, max_depth: int, came
     prim = np.zeros((height, width), np.uint32)
     check(lib.pt_render(scene.handle, C.byref(rd), rgb.ctypes.data, prim.ctypes.data, 0, None))
     return rgb, prim
+
+
+def film_to_rgba8(rgb_dev_ptr: int, width: int, height: int) -> np.ndarray:
+    """A device film (width*height*3 floats at rgb_dev_ptr) as the reference's PNG bytes:
+    (height, width, 4) uint8, quantised on the device."""
+    out = np.zeros((height, width, 4), np.uint8)
+    check(lib.pt_film_to_rgba8(rgb_dev_ptr, width, height, out.ctypes.data, 0, None))
+    return out
+
+
+def write_png(path: str, rgba: np.ndarray):
+    """RGBA8 pixels (H, W, 4) to a PNG file."""
+    rgba = np.ascontiguousarray(rgba, np.uint8)
+    check(lib.pt_write_png(str(path).encode(), rgba.ctypes.data, rgba.shape[1], rgba.shape[0]))
 
 
 class GpuRunner:

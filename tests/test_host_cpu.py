@@ -202,3 +202,42 @@ def test_f64_emulation_double_rounding_ties():
     q = np.array(rows, np.float32)
     got = np.array([pb.f64_diff_emulated_host(*map(float, r)) for r in q], np.float32)
     assert_bit_equal(got, f64_reference(q), "double rounding")
+
+
+def _read_png(path):
+    """Minimal PNG reader for the test: chunks with CRC check, zlib inflate, filter-0 scanlines."""
+    import struct
+    import zlib
+    data = open(path, "rb").read()
+    assert data[:8] == b"\x89PNG\r\n\x1a\n"
+    pos, chunks = 8, []
+    while pos < len(data):
+        n = struct.unpack(">I", data[pos:pos + 4])[0]
+        typ, body = data[pos + 4:pos + 8], data[pos + 8:pos + 8 + n]
+        crc = struct.unpack(">I", data[pos + 8 + n:pos + 12 + n])[0]
+        assert zlib.crc32(typ + body) & 0xFFFFFFFF == crc
+        chunks.append((typ, body))
+        pos += 12 + n
+    assert [c[0] for c in chunks] == [b"IHDR", b"IDAT", b"IEND"]
+    w, h, depth, ctype = struct.unpack(">IIBB", chunks[0][1][:10])
+    assert (depth, ctype) == (8, 6)
+    raw = zlib.decompress(chunks[1][1])
+    rows = np.frombuffer(raw, np.uint8).reshape(h, 1 + 4 * w)
+    assert (rows[:, 0] == 0).all()
+    return rows[:, 1:].reshape(h, w, 4)
+
+
+@pytest.mark.parametrize("w,h", [(1, 1), (37, 5), (300, 250)])
+def test_png_writer_round_trip(tmp_path, w, h):
+    rng = np.random.default_rng(w * 7 + h)
+    rgba = rng.integers(0, 256, (h, w, 4), dtype=np.uint8)
+    path = tmp_path / "film.png"
+    pb.write_png(path, rgba)
+    assert np.array_equal(_read_png(path), rgba)
+
+
+def test_png_quantisation_oracle_known_answers():
+    # PNGFilm::Output: clamp at 255, truncate toward zero, alpha 255
+    rgb = np.array([[[0.0, 0.5, 254.99], [255.0, 300.0, 1e9], [1.0, 127.9999, 128.0]]], np.float32)
+    exp = np.array([[[0, 0, 254, 255], [255, 255, 255, 255], [1, 127, 128, 255]]], np.uint8)
+    assert np.array_equal(po.film_to_rgba8(rgb), exp)

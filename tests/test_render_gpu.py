@@ -97,3 +97,29 @@ def test_runner_interface(cuda_device):
     r.run()
     rgb, prim = r.output()
     assert rgb.shape == (24, 32, 3) and prim.shape == (24, 32)
+
+
+def test_film_to_rgba8_matches_reference_quantisation(cuda_device):
+    import ctypes as C
+    import torch
+    rng = np.random.default_rng(3)
+    h, w = 37, 53
+    rgb = rng.uniform(0, 300, (h, w, 3)).astype(np.float32)
+    rgb[0, 0] = (0.0, 0.5, 254.99)
+    rgb[0, 1] = (255.0, 1e9, 127.9999)
+    exp = po.film_to_rgba8(rgb)
+    d = torch.from_numpy(rgb).cuda()
+    assert_bit_equal(pb.film_to_rgba8(d.data_ptr(), w, h), exp, "rgba8, host output")
+    out = torch.zeros(h * w * 4, dtype=torch.uint8, device="cuda")
+    pb.check(pb.lib.pt_film_to_rgba8(d.data_ptr(), w, h, out.data_ptr(), pb.MEM_DEVICE, None))
+    torch.cuda.synchronize()
+    assert_bit_equal(out.cpu().numpy().reshape(h, w, 4), exp, "rgba8, device output")
+    # a rendered film, quantised on the device, equals the oracle's quantisation of the same film
+    meshes, env = W.small_scene(level=3)
+    scene = pb.Scene(meshes, env)
+    rd = pb.render_desc(64, 48, 4, 4, W.SMALL_CAMERA, 5, pb.RENDER_NEE)
+    film = torch.zeros(64 * 48 * 3, dtype=torch.float32, device="cuda")
+    pb.check(pb.lib.pt_render(scene.handle, C.byref(rd), film.data_ptr(), None, pb.MEM_DEVICE, None))
+    torch.cuda.synchronize()
+    host_film = film.cpu().numpy().reshape(48, 64, 3)
+    assert_bit_equal(pb.film_to_rgba8(film.data_ptr(), 64, 48), po.film_to_rgba8(host_film), "rendered film")
