@@ -234,6 +234,25 @@ int pt_render(pt_scene *scene, const pt_render_desc *desc, float *rgb_out,
 int pt_render_noalloc(pt_scene *scene, const pt_render_desc *desc, float *rgb_dev,
                       uint32_t *primary_dev, void *stream);
 
+/* ---- scene ingest ------------------------------------------------------------------------- */
+
+/* A mesh read from a file: packed vertex arrays and faces, the shape pt_mesh_desc takes (and the
+ * reference's mesh_geometry x/y/z_packed, nx/ny/nz_packed, u/v_packed, fv0/fv1/fv2, mesh.h:37-62).
+ * Arrays are owned by the library; release them with pt_mesh_data_free. */
+typedef struct pt_mesh_data {
+    float    *x, *y, *z;
+    uint32_t  num_vertices;
+    uint32_t *fv0, *fv1, *fv2;
+    uint32_t  num_faces;
+    float    *nx, *ny, *nz;   /* NULL when the file has no vertex normals */
+    float    *u, *v;          /* NULL when the file has no vertex uv */
+} pt_mesh_data;
+
+/* ply_parser::parse_file (src/common/parsers/mesh_parsers.cpp:336-545): ascii and binary PLY.
+ * Header errors and malformed data return PT_EINVAL with the reason. */
+int pt_load_ply(const char *path, pt_mesh_data *out);
+void pt_mesh_data_free(pt_mesh_data *mesh);
+
 /* ---- output format ------------------------------------------------------------------------ */
 
 /* The film as the reference's PNG output stores it: RGBA8, row-major, each channel

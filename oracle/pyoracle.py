@@ -322,3 +322,17 @@ def film_to_rgba8(rgb: np.ndarray) -> np.ndarray:
     out = np.zeros((h, w, 4), np.uint8)
     oracle_lib().orc_film_to_rgba8(_f(rgb), h * w, out.ctypes.data)
     return out
+
+
+def ref_load_ply(path: str):
+    """The reference's own ply_parser::parse_file (oracle/_ref): (x, y, z, faces, normals or None)."""
+    lib = ref_lib()
+    f = lib.ref_load_ply
+    f.argtypes = [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_int)] + [C.c_void_p] * 9
+    nv, nf, hn = C.c_uint32(0), C.c_uint32(0), C.c_int(0)
+    f(str(path).encode(), C.byref(nv), C.byref(nf), C.byref(hn), *([None] * 9))
+    a = [np.zeros(nv.value, np.float32) for _ in range(6)]
+    fv = [np.zeros(nf.value, np.uint32) for _ in range(3)]
+    f(str(path).encode(), C.byref(nv), C.byref(nf), C.byref(hn), *[v.ctypes.data for v in a + fv])
+    normals = np.stack(a[3:], 1) if hn.value else None
+    return a[0], a[1], a[2], np.stack(fv, 1), normals

@@ -29,6 +29,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "common/parsers/mesh_parsers.h"
 #include "cpu/acceleration/bvh.h"
 #include "cpu/cameras/PerspectiveCamera.h"
 #include "cpu/shading/brdf/mirror_brdf.h"
@@ -56,6 +57,10 @@ void Logger::info(const std::string&) {}
 void Logger::warning(const std::string&) {}
 void Logger::error(const std::string& text) { std::fprintf(stderr, "%s\n", text.c_str()); }
 }  // namespace poly
+// Path globals of src/common/utilities/GlobalDefines.h (a header the reference's main.cpp
+// includes once); the parsers below only see absolute paths.
+std::string UnixPathSeparator = "/";
+std::string GetCurrentWorkingDirectory() { return std::string("/"); }
 thread_local poly::stats thread_stats;
 poly::stats main_stats;
 
@@ -504,6 +509,32 @@ void ref_render_rows(void* p, const ref_render_desc* rd, uint32_t row_begin, uin
             rgb[3 * pix + 2] = accum.b;
         }
     });
+}
+
+// ply_parser::parse_file on one file (the reference's own PLY reader).  Counts are returned
+// first (pass NULL arrays); a second call copies the packed arrays out.
+int ref_load_ply(const char* path, uint32_t* num_vertices, uint32_t* num_faces, int* has_normals, float* x, float* y,
+                 float* z, float* nx, float* ny, float* nz, uint32_t* fv0, uint32_t* fv1, uint32_t* fv2) {
+    auto g = std::make_shared<poly::mesh_geometry>();
+    const poly::ply_parser parser;
+    parser.parse_file(g, path);
+    *num_vertices = (uint32_t)g->x_packed.size();
+    *num_faces = (uint32_t)g->fv0.size();
+    *has_normals = g->has_vertex_normals ? 1 : 0;
+    if (x) {
+        std::memcpy(x, g->x_packed.data(), 4 * g->x_packed.size());
+        std::memcpy(y, g->y_packed.data(), 4 * g->y_packed.size());
+        std::memcpy(z, g->z_packed.data(), 4 * g->z_packed.size());
+        std::memcpy(fv0, g->fv0.data(), 4 * g->fv0.size());
+        std::memcpy(fv1, g->fv1.data(), 4 * g->fv1.size());
+        std::memcpy(fv2, g->fv2.data(), 4 * g->fv2.size());
+        if (g->has_vertex_normals && nx) {
+            std::memcpy(nx, g->nx_packed.data(), 4 * g->nx_packed.size());
+            std::memcpy(ny, g->ny_packed.data(), 4 * g->ny_packed.size());
+            std::memcpy(nz, g->nz_packed.data(), 4 * g->nz_packed.size());
+        }
+    }
+    return 0;
 }
 
 }  // extern "C"

@@ -113,6 +113,12 @@ class ServerConfig(C.Structure):
                 ("tuning", BatchTuning), ("policy", C.c_uint32), ("host_budget", C.c_uint64)]
 
 
+class MeshData(C.Structure):
+    _fields_ = [("x", _fp), ("y", _fp), ("z", _fp), ("num_vertices", C.c_uint32),
+                ("fv0", _up), ("fv1", _up), ("fv2", _up), ("num_faces", C.c_uint32),
+                ("nx", _fp), ("ny", _fp), ("nz", _fp), ("u", _fp), ("v", _fp)]
+
+
 class RequestTiming(C.Structure):
     _fields_ = [("admitted_ms", C.c_double), ("first_wave_ms", C.c_double), ("last_wave_ms", C.c_double),
                 ("done_ms", C.c_double)]
@@ -144,6 +150,8 @@ def _load() -> C.CDLL:
         "pt_trace_autotune": (i, [_vp, _vp, u64, _vp, C.POINTER(TraceTuning), C.POINTER(C.c_float)]),
         "pt_render_noalloc": (i, [_vp, C.POINTER(RenderDesc), _vp, _vp, _vp]),
         "pt_film_to_rgba8": (i, [_vp, u32, u32, _vp, u32, _vp]),
+        "pt_load_ply": (i, [C.c_char_p, C.POINTER(MeshData)]),
+        "pt_mesh_data_free": (None, [C.POINTER(MeshData)]),
         "pt_write_png": (i, [C.c_char_p, _vp, u32, u32]),
         "pt_batch_default_tuning": (i, [C.POINTER(BatchTuning)]),
         "pt_batch_create": (i, [C.POINTER(BatchItem), u32, C.POINTER(BatchTuning), C.POINTER(_vp)]),
@@ -365,6 +373,25 @@ def render(scene: Scene, width: int, height: int, spp: int, max_depth: int, came
     prim = np.zeros((height, width), np.uint32)
     check(lib.pt_render(scene.handle, C.byref(rd), rgb.ctypes.data, prim.ctypes.data, 0, None))
     return rgb, prim
+
+
+def load_ply(path: str, **mesh_kwargs) -> Mesh:
+    """A PLY file as a Mesh (pt_load_ply); keyword arguments go to Mesh (transform, material...).
+    Vertex uv, when present, is in the returned mesh's `uv` attribute."""
+    d = MeshData()
+    check(lib.pt_load_ply(str(path).encode(), C.byref(d)))
+    try:
+        nv, nf = d.num_vertices, d.num_faces
+        arr = lambda p, n, dt: np.ctypeslib.as_array(p, (n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
+        x, y, z = (arr(getattr(d, k), nv, np.float32) for k in ("x", "y", "z"))
+        faces = np.stack([arr(getattr(d, k), nf, np.uint32) for k in ("fv0", "fv1", "fv2")], 1) if nf else np.zeros((0, 3), np.uint32)
+        normals = np.stack([arr(getattr(d, k), nv, np.float32) for k in ("nx", "ny", "nz")], 1) if bool(d.nx) else None
+        uv = np.stack([arr(getattr(d, k), nv, np.float32) for k in ("u", "v")], 1) if bool(d.u) else None
+    finally:
+        lib.pt_mesh_data_free(C.byref(d))
+    m = Mesh(x, y, z, faces, normals=normals, **mesh_kwargs)
+    m.uv = uv
+    return m
 
 
 def film_to_rgba8(rgb_dev_ptr: int, width: int, height: int) -> np.ndarray:
