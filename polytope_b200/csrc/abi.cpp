@@ -80,14 +80,16 @@ bool is_pinned(const void* p) {
 }
 
 constexpr size_t kChunkRays = size_t(1) << 20;
+constexpr int kSlots = 4;  // chunks in flight: one being copied in, one or two in kernels, one copied out
 
 int ensure_staging(pt_scene* s) {
     if (s->staging_rays) return PT_OK;
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < 4; ++i) {
         PT_CUDA(cudaStreamCreateWithFlags((cudaStream_t*)&s->streams[i], cudaStreamNonBlocking));
     }
-    for (int i = 0; i < 4; ++i) PT_CUDA(cudaEventCreateWithFlags((cudaEvent_t*)&s->events[i], cudaEventDisableTiming));
-    const size_t in_b = 2 * kChunkRays * sizeof(pt_ray), out_b = 2 * kChunkRays * sizeof(pt_hit);
+    for (int i = 0; i < 3 * kSlots + 1; ++i)
+        PT_CUDA(cudaEventCreateWithFlags((cudaEvent_t*)&s->events[i], cudaEventDisableTiming));
+    const size_t in_b = kSlots * kChunkRays * sizeof(pt_ray), out_b = kSlots * kChunkRays * sizeof(pt_hit);
     if (cudaMalloc(&s->dev_in, in_b) != cudaSuccess || cudaMalloc(&s->dev_out, out_b) != cudaSuccess)
         return fail(PT_ENOMEM, "cudaMalloc staging buffers");
     if (cudaMallocHost(&s->pin_in, in_b) != cudaSuccess || cudaMallocHost(&s->pin_out, out_b) != cudaSuccess)
@@ -133,76 +135,87 @@ int scene_trace(pt_scene* s, const pt_ray* rays, uint64_t n, pt_hit* hits, uint3
         if (e != cudaSuccess) return cuda_fail(e, "trace kernel launch");
         return PT_OK;
     }
-    // Host pointers: pipeline chunks over two streams so copies overlap the kernels.
+    // Host pointers: 1 M-ray chunks through kSlots staging slots and three engines at once -- a
+    // stream of host->device copies, two kernel streams (so one chunk's kernel tail overlaps the
+    // next), and a stream of device->host copies -- ordered per slot by events.  Pageable arrays
+    // go through the pinned staging of their slot.
     std::lock_guard<std::mutex> lock(s->staging_mu);
     int rc = ensure_staging(s);
     if (rc) return rc;
-    cudaStream_t st[2] = {(cudaStream_t)s->streams[0], (cudaStream_t)s->streams[1]};
-    cudaEvent_t done[2] = {(cudaEvent_t)s->events[0], (cudaEvent_t)s->events[1]};
-    cudaEvent_t dep = (cudaEvent_t)s->events[2];
+    cudaStream_t h2d = (cudaStream_t)s->streams[0], d2h = (cudaStream_t)s->streams[3];
+    cudaStream_t kst[2] = {(cudaStream_t)s->streams[1], (cudaStream_t)s->streams[2]};
+    cudaEvent_t* ev = (cudaEvent_t*)s->events;
+    cudaEvent_t *ev_in = ev, *ev_k = ev + kSlots, *ev_out = ev + 2 * kSlots, dep = ev[3 * kSlots];
     PT_CUDA(cudaEventRecord(dep, (cudaStream_t)stream));
-    PT_CUDA(cudaStreamWaitEvent(st[0], dep, 0));
-    PT_CUDA(cudaStreamWaitEvent(st[1], dep, 0));
-    PT_CUDA(cudaMemsetAsync(s->err_flag, 0, sizeof(int), st[0]));
-    PT_CUDA(cudaStreamSynchronize(st[0]));
+    for (int i = 0; i < 4; ++i) PT_CUDA(cudaStreamWaitEvent((cudaStream_t)s->streams[i], dep, 0));
+    PT_CUDA(cudaMemsetAsync(s->err_flag, 0, sizeof(int), h2d));  // before every copy-in, so before every kernel
     const bool pin_rays = is_pinned(rays), pin_hits = is_pinned(hits);
     const bool counted = node_tests || tri_tests;
-    std::vector<uint32_t> dev_counts_host;
     uint32_t* dcounts = nullptr;
-    if (counted) {
-        if (cudaMalloc(&dcounts, 2 * sizeof(uint32_t) * kChunkRays * 2) != cudaSuccess)
-            return fail(PT_ENOMEM, "cudaMalloc count buffers");
-    }
+    if (counted && cudaMalloc(&dcounts, 2 * sizeof(uint32_t) * n) != cudaSuccess)
+        return fail(PT_ENOMEM, "cudaMalloc count buffers");
+    struct Free { uint32_t* p; ~Free() { if (p) cudaFree(p); } } free_counts{dcounts};
     const uint64_t nchunks = (n + kChunkRays - 1) / kChunkRays;
-    uint64_t pending[2] = {~0ull, ~0ull};  // chunk whose results sit in each slot
-    auto drain = [&](int slot) -> int {
-        if (pending[slot] == ~0ull) return PT_OK;
-        PT_CUDA(cudaEventSynchronize(done[slot]));
-        const uint64_t c = pending[slot];
-        const uint64_t off = c * kChunkRays, cnt = std::min<uint64_t>(kChunkRays, n - off);
-        if (!pin_hits)
+    uint64_t in_slot[kSlots];
+    for (int k = 0; k < kSlots; ++k) in_slot[k] = ~0ull;  // chunk whose data occupies each slot
+    auto drain = [&](int slot) -> int {  // pageable hits: move the slot's results out
+        if (in_slot[slot] == ~0ull) return PT_OK;
+        PT_CUDA(cudaEventSynchronize(ev_out[slot]));
+        if (!pin_hits) {
+            const uint64_t off = in_slot[slot] * kChunkRays, cnt = std::min<uint64_t>(kChunkRays, n - off);
             std::memcpy(hits + off, (pt_hit*)s->pin_out + slot * kChunkRays, cnt * sizeof(pt_hit));
-        if (counted) {
-            std::vector<uint32_t> tmp(2 * cnt);
-            PT_CUDA(cudaMemcpy(tmp.data(), dcounts + slot * 2 * kChunkRays, 2 * cnt * sizeof(uint32_t),
-                               cudaMemcpyDeviceToHost));
-            if (node_tests) std::memcpy(node_tests + off, tmp.data(), cnt * sizeof(uint32_t));
-            if (tri_tests) std::memcpy(tri_tests + off, tmp.data() + cnt, cnt * sizeof(uint32_t));
         }
-        pending[slot] = ~0ull;
+        in_slot[slot] = ~0ull;
         return PT_OK;
     };
     for (uint64_t c = 0; c < nchunks; ++c) {
-        const int slot = (int)(c & 1);
-        rc = drain(slot);
-        if (rc) { if (dcounts) cudaFree(dcounts); return rc; }
+        const int slot = (int)(c % kSlots);
+        const bool reused = in_slot[slot] != ~0ull;
+        if (reused && !pin_hits) {
+            rc = drain(slot);
+            if (rc) return rc;
+        }
         const uint64_t off = c * kChunkRays, cnt = std::min<uint64_t>(kChunkRays, n - off);
         pt_ray* din = (pt_ray*)s->dev_in + slot * kChunkRays;
         pt_hit* dout = (pt_hit*)s->dev_out + slot * kChunkRays;
         const void* src = rays + off;
         if (!pin_rays) {
+            if (reused) PT_CUDA(cudaEventSynchronize(ev_in[slot]));  // the slot's previous copy-in has read it
             std::memcpy((pt_ray*)s->pin_in + slot * kChunkRays, rays + off, cnt * sizeof(pt_ray));
             src = (pt_ray*)s->pin_in + slot * kChunkRays;
         }
-        PT_CUDA(cudaMemcpyAsync(din, src, cnt * sizeof(pt_ray), cudaMemcpyHostToDevice, st[slot]));
+        if (reused) PT_CUDA(cudaStreamWaitEvent(h2d, ev_k[slot], 0));  // din is free once its kernel ran
+        PT_CUDA(cudaMemcpyAsync(din, src, cnt * sizeof(pt_ray), cudaMemcpyHostToDevice, h2d));
+        PT_CUDA(cudaEventRecord(ev_in[slot], h2d));
+        cudaStream_t k = kst[c & 1];
+        PT_CUDA(cudaStreamWaitEvent(k, ev_in[slot], 0));
+        if (reused) PT_CUDA(cudaStreamWaitEvent(k, ev_out[slot], 0));  // dout is free once copied out
         a.rays = din;
         a.hits = dout;
         a.n = cnt;
         a.counter = next_counter();
-        a.node_tests = counted ? dcounts + slot * 2 * kChunkRays : nullptr;
-        a.tri_tests = counted ? dcounts + slot * 2 * kChunkRays + cnt : nullptr;
-        cudaError_t e = launch_trace(a, st[slot]);
-        if (e != cudaSuccess) { if (dcounts) cudaFree(dcounts); return cuda_fail(e, "trace kernel launch"); }
+        a.node_tests = counted ? dcounts + off : nullptr;
+        a.tri_tests = counted ? dcounts + n + off : nullptr;
+        cudaError_t e = launch_trace(a, k);
+        if (e != cudaSuccess) return cuda_fail(e, "trace kernel launch");
+        PT_CUDA(cudaEventRecord(ev_k[slot], k));
+        PT_CUDA(cudaStreamWaitEvent(d2h, ev_k[slot], 0));
         void* dst = pin_hits ? (void*)(hits + off) : (void*)((pt_hit*)s->pin_out + slot * kChunkRays);
-        PT_CUDA(cudaMemcpyAsync(dst, dout, cnt * sizeof(pt_hit), cudaMemcpyDeviceToHost, st[slot]));
-        PT_CUDA(cudaEventRecord(done[slot], st[slot]));
-        pending[slot] = c;
+        PT_CUDA(cudaMemcpyAsync(dst, dout, cnt * sizeof(pt_hit), cudaMemcpyDeviceToHost, d2h));
+        PT_CUDA(cudaEventRecord(ev_out[slot], d2h));
+        in_slot[slot] = c;
     }
-    for (int slot = 0; slot < 2; ++slot) {
-        rc = drain(slot);
-        if (rc) { if (dcounts) cudaFree(dcounts); return rc; }
+    for (uint64_t c = nchunks > kSlots ? nchunks - kSlots : 0; c < nchunks; ++c) {
+        rc = drain((int)(c % kSlots));
+        if (rc) return rc;
     }
-    if (dcounts) cudaFree(dcounts);
+    PT_CUDA(cudaStreamSynchronize(d2h));
+    if (counted) {
+        std::vector<uint32_t> tmp(2 * n);
+        PT_CUDA(cudaMemcpy(tmp.data(), dcounts, 2 * n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+        if (node_tests) std::memcpy(node_tests, tmp.data(), n * sizeof(uint32_t));
+        if (tri_tests) std::memcpy(tri_tests, tmp.data() + n, n * sizeof(uint32_t));
+    }
     int err = 0;
     PT_CUDA(cudaMemcpy(&err, s->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) return fail(PT_ESTACK, "a ray exceeded the traversal stack (malformed or too deep tree)");

@@ -105,8 +105,8 @@ struct pt_scene {
     void* dev_in = nullptr;
     void* dev_out = nullptr;
     size_t staging_rays = 0;
-    void* streams[2] = {nullptr, nullptr};
-    void* events[4] = {nullptr, nullptr, nullptr, nullptr};
+    void* streams[4] = {};  // host-pointer traces: copies in, two kernel streams, copies out
+    void* events[16] = {};
     void* err_flag = nullptr;  // device int, set when a kernel hit a guard
     // ray counters of the persistent trace kernel: one per launch in flight, taken round-robin
     void* ray_counters = nullptr;
