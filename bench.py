@@ -376,7 +376,9 @@ def run_reference(args, rank, world):
         "impl": "reference", "metric": "Mrays/s", "value": round(value, 4), "unit": "Mrays/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "rays_per_step": sample, "threads": threads},
+        "config": {"workload": WORKLOAD, "rays_per_gpu": N_RAYS, "faces": int(sum(len(m.faces) for m in meshes)),
+                   "launch": f"the reference's own bvh::intersect_compact + Mesh::intersect ({kind}), host threads",
+                   "parallelism": f"host threads x{threads}", "sample_rays_per_step": sample},
         "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": threads, "kind": kind,
                          "sample": f"first {sample} rays of the {N_RAYS}-ray set per step, all host threads"},
         "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
