@@ -449,7 +449,9 @@ def f64_diff_emulated_host(a: float, b: float, c: float, d: float) -> float:
 
 
 def selftest_device(which: int, inp: np.ndarray, n: int, seed: int = 0) -> np.ndarray:
-    if which == 0:
+    if which == 3:
+        out = np.zeros(n, np.uint32)
+    elif which == 0:
         out = np.zeros(n, np.float32)
     elif which == 1:
         out = np.zeros((n, 2), np.float32)

@@ -481,8 +481,9 @@ int pt_selftest_device(int which, const void* in, void* out, uint32_t n, uint64_
         cudaGetLastError();
         return fail(PT_ECUDA, "no CUDA device available");
     }
-    const size_t in_b = (which == 1) ? 4 * n : 16 * (size_t)n;
-    const size_t out_b = (which == 0) ? 4 * (size_t)n : (which == 1 ? 8 * (size_t)n : 16 * (size_t)n);
+    if (which < 0 || which > 3) return fail(PT_EINVAL, "unknown selftest");
+    const size_t in_b = which == 1 ? 4 * (size_t)n : (which == 3 ? 64 * (size_t)n : 16 * (size_t)n);
+    const size_t out_b = (which == 0 || which == 3) ? 4 * (size_t)n : (which == 1 ? 8 * (size_t)n : 16 * (size_t)n);
     void *din = nullptr, *dout = nullptr;
     if (cudaMalloc(&din, in_b) != cudaSuccess || cudaMalloc(&dout, out_b) != cudaSuccess) {
         if (din) cudaFree(din);
@@ -492,7 +493,8 @@ int pt_selftest_device(int which, const void* in, void* out, uint32_t n, uint64_
     cudaError_t e;
     if (which == 0) e = launch_selftest_f64((const float*)din, (float*)dout, n, 0);
     else if (which == 1) e = launch_selftest_sincos((const float*)din, (float*)dout, n, 0);
-    else e = launch_selftest_philox((const uint32_t*)din, (uint32_t*)dout, n, seed, 0);
+    else if (which == 2) e = launch_selftest_philox((const uint32_t*)din, (uint32_t*)dout, n, seed, 0);
+    else e = launch_selftest_box((const float*)din, (uint32_t*)dout, n, 0);
     if (e == cudaSuccess) e = cudaMemcpy(out, dout, out_b, cudaMemcpyDeviceToHost);
     cudaFree(din);
     cudaFree(dout);

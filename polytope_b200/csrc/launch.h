@@ -28,5 +28,7 @@ cudaError_t launch_trace(const TraceArgs& a, cudaStream_t s);
 cudaError_t launch_selftest_f64(const float* in4, float* out, uint32_t n, cudaStream_t s);
 cudaError_t launch_selftest_sincos(const float* u, float* out2, uint32_t n, cudaStream_t s);
 cudaError_t launch_selftest_philox(const uint32_t* in4, uint32_t* out4, uint32_t n, uint64_t seed, cudaStream_t s);
+// Box test as the traversal kernels run it: in16 = {bb[6], org[3], dir[3], tmax, 0, 0, 0}.
+cudaError_t launch_selftest_box(const float* in16, uint32_t* hit, uint32_t n, cudaStream_t s);
 
 }  // namespace pt

@@ -183,6 +183,21 @@ __global__ void selftest_philox_kernel(const uint4* in, uint4* out, uint32_t n, 
     out[i] = make_uint4(c[0], c[1], c[2], c[3]);
 }
 
+__global__ void selftest_box_kernel(const float* in, uint32_t* out, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* c = in + 16 * (size_t)i;
+    RayState r;
+    ray_setup(r, c[6], c[7], c[8], c[9], c[10], c[11]);
+    out[i] = box_hits(r, c[0], c[1], c[2], c[3], c[4], c[5], c[12], needs_inside_test(r, c[12])) ? 1u : 0u;
+}
+
+cudaError_t launch_selftest_box(const float* in16, uint32_t* hit, uint32_t n, cudaStream_t s) {
+    if (!n) return cudaSuccess;
+    selftest_box_kernel<<<(n + 127) / 128, 128, 0, s>>>(in16, hit, n);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_selftest_f64(const float* in4, float* out, uint32_t n, cudaStream_t s) {
     if (!n) return cudaSuccess;
     selftest_f64_kernel<<<(n + 127) / 128, 128, 0, s>>>((const float4*)in4, out, n);

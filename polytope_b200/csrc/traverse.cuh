@@ -54,11 +54,22 @@ PT_HD void ray_setup(RayState& r, float ox, float oy, float oz, float dx, float 
     r.sz = frcp(dkz);
 }
 
+// Whether box_hits must evaluate the reference's "origin strictly inside" early-out.  For a ray
+// whose far bound is not negative and whose 1/d has no NaN, an origin strictly inside the box
+// always passes the slab test too (each axis then has one non-positive and one non-negative bound,
+// or infinite ones, so near stays 0 <= far), so the early-out cannot change the result and is
+// skipped.  The running MinT only ever drops to accepted t > 0, so this holds for the whole walk.
+PT_HD bool needs_inside_test(const RayState& r, float tmax) {
+    return !(tmax >= 0.f) || r.ix != r.ix || r.iy != r.iy || r.iz != r.iz;
+}
+
 // BoundingBox::Hits with the running MinT as the far bound.
 PT_HD bool box_hits(const RayState& r, float b0, float b1, float b2, float b3, float b4, float b5,
-                                         float min_t) {
-    const bool inside = r.ox > b0 && r.ox < b3 && r.oy > b1 && r.oy < b4 && r.oz > b2 && r.oz < b5;
-    if (inside) return true;
+                                         float min_t, bool check_inside = true) {
+    if (check_inside) {
+        const bool inside = r.ox > b0 && r.ox < b3 && r.oy > b1 && r.oy < b4 && r.oz > b2 && r.oz < b5;
+        if (inside) return true;
+    }
     const float gm = bitsf(PT_GAMMA_MUL_BITS);
     float far_t = min_t, near_t = 0.f;
     float tn = fmul(fsub(b0, r.ox), r.ix), tf = fmul(fsub(b3, r.ox), r.ix);
@@ -179,6 +190,7 @@ struct RayWalkT {
     float u, v, w;
     uint32_t nodes, tris;
     bool any, done;
+    bool check_inside;  // needs_inside_test for this ray
     int sp;
     WalkStack<CAP, SH> stack;
 };
@@ -187,6 +199,7 @@ using RayWalk = RayWalkT<>;
 template <int CAP, int SH>
 PT_HD void walk_begin(RayWalkT<CAP, SH>& k, float ox, float oy, float oz, float dx, float dy, float dz, float tmax, bool any) {
     ray_setup(k.r, ox, oy, oz, dx, dy, dz);
+    k.check_inside = needs_inside_test(k.r, tmax);
     k.min_t = tmax;
     k.prim = kPrimNone;
     k.leaf = kPrimNone;
@@ -211,7 +224,8 @@ PT_HD bool walk_to_leaf(RayWalkT<CAP, SH>& k, const uint4* __restrict__ nodes, u
         const uint4 a = ldg(nodes + 2 * (size_t)ni);
         const uint4 b = ldg(nodes + 2 * (size_t)ni + 1);
         if (COUNT) k.nodes++;
-        if (!box_hits(k.r, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), k.min_t)) continue;
+        if (!box_hits(k.r, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), k.min_t, k.check_inside))
+            continue;
         const uint32_t nf = b.w & 0xFFFFu;
         if (nf > 0) {
             leaf_off = b.z;
@@ -268,6 +282,7 @@ PT_HD TraceResult traverse(const uint4* __restrict__ nodes, const float4* __rest
     res.nodes = res.tris = 0;
     res.overflow = false;
     const bool neg_x = r.ix < 0, neg_y = r.iy < 0, neg_z = r.iz < 0;
+    const bool check_inside = needs_inside_test(r, tmax);
     uint32_t stack[CAP];
     int sp = 0;
     stack[sp++] = 0;
@@ -279,7 +294,7 @@ PT_HD TraceResult traverse(const uint4* __restrict__ nodes, const float4* __rest
         const uint4 b = ldg(nodes + 2 * (size_t)ni + 1);
         if (COUNT) res.nodes++;
         if (!box_hits(r, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w),
-                      bitsf(b.x), bitsf(b.y), min_t))
+                      bitsf(b.x), bitsf(b.y), min_t, check_inside))
             continue;
         const uint32_t nf = b.w & 0xFFFFu;
         if (nf > 0) {

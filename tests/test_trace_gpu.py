@@ -38,6 +38,31 @@ def test_exact_helpers_on_device(cuda_device):
     assert (dev[:256] == host).all()
 
 
+def test_box_test_on_device_matches_reference_semantics(cuda_device):
+    """BoundingBox::Hits with its inside early-out, against the device test that skips the early-out
+    when it cannot change the answer: origins inside, outside and on faces; zero, negative-zero and
+    NaN direction components; tmax of inf, 0, positive, negative and NaN."""
+    rng = np.random.default_rng(17)
+    n = 20000
+    lo = rng.uniform(-2, 1, (n, 3)).astype(np.float32)
+    hi = (lo + rng.uniform(0, 2, (n, 3))).astype(np.float32)
+    o = rng.uniform(-3, 3, (n, 3)).astype(np.float32)
+    inside = rng.random(n) < 0.3
+    o[inside] = ((lo + hi) / 2)[inside]
+    on_face = rng.random(n) < 0.1
+    o[on_face, 0] = lo[on_face, 0]
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d[rng.random(n) < 0.1, 1] = 0.0
+    d[rng.random(n) < 0.05, 2] = -0.0
+    d[rng.random(n) < 0.01, 0] = np.nan
+    tmax = rng.choice(np.array([np.inf, 0.0, 1.5, 100.0, -1.0, np.nan], np.float32), n).astype(np.float32)
+    case = np.zeros((n, 16), np.float32)
+    case[:, 0:3], case[:, 3:6], case[:, 6:9], case[:, 9:12], case[:, 12] = lo, hi, o, d, tmax
+    got = pb.selftest_device(3, case, n)
+    exp = np.array([po.bbox_hits("orc", np.concatenate([lo[i], hi[i]]), o[i], d[i], float(tmax[i])) for i in range(n)])
+    assert (got.astype(bool) == exp).all(), np.nonzero(got.astype(bool) != exp)[0][:10]
+
+
 def test_small_scene_random_rays_match_fixture_and_oracle(cuda_device):
     g = load_golden("small_scene.npz")
     meshes, env = W.small_scene()
