@@ -63,7 +63,9 @@ PT_HD bool needs_inside_test(const RayState& r, float tmax) {
     return !(tmax >= 0.f) || r.ix != r.ix || r.iy != r.iy || r.iz != r.iz;
 }
 
-// BoundingBox::Hits with the running MinT as the far bound.
+// BoundingBox::Hits with the running MinT as the far bound.  The reference returns false as soon
+// as near > far after an axis; near only grows and far only shrinks (a NaN bound leaves either
+// unchanged), so testing once after the third axis gives the same answer without two branches.
 PT_HD bool box_hits(const RayState& r, float b0, float b1, float b2, float b3, float b4, float b5,
                                          float min_t, bool check_inside = true) {
     if (check_inside) {
@@ -79,7 +81,6 @@ PT_HD bool box_hits(const RayState& r, float b0, float b1, float b2, float b3, f
     tf = fmul(tf, gm);
     near_t = (tn > near_t) ? tn : near_t;
     far_t = (tf < far_t) ? tf : far_t;
-    if (near_t > far_t) return false;
     tn = fmul(fsub(b1, r.oy), r.iy); tf = fmul(fsub(b4, r.oy), r.iy);
     sw = tn;
     tn = tn > tf ? tf : tn;
@@ -87,7 +88,6 @@ PT_HD bool box_hits(const RayState& r, float b0, float b1, float b2, float b3, f
     tf = fmul(tf, gm);
     near_t = (tn > near_t) ? tn : near_t;
     far_t = (tf < far_t) ? tf : far_t;
-    if (near_t > far_t) return false;
     tn = fmul(fsub(b2, r.oz), r.iz); tf = fmul(fsub(b5, r.oz), r.iz);
     sw = tn;
     tn = tn > tf ? tf : tn;
