@@ -53,6 +53,18 @@ PT_HD T ldg(const T* p) {
     return *p;
 #endif
 }
+// One 32-byte node record (two uint4) with a single 256-bit read-only load on the device; the
+// record must be 32-byte aligned (node arrays are cudaMalloc'd and nodes are 32 bytes).
+PT_HD void ldg_node(const uint4* p, uint4& a, uint4& b) {
+#ifdef __CUDA_ARCH__
+    asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+        : "l"(p));
+#else
+    a = p[0];
+    b = p[1];
+#endif
+}
 PT_HD void raise_flag(int* flag) {
 #ifdef __CUDA_ARCH__
     atomicExch(flag, 1);

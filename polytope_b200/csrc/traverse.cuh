@@ -221,8 +221,8 @@ PT_HD bool walk_to_leaf(RayWalkT<CAP, SH>& k, const uint4* __restrict__ nodes, u
     while (k.sp > 0) {
         const uint32_t ni = k.stack.get(--k.sp);
         if (ni >= num_nodes) return false;
-        const uint4 a = ldg(nodes + 2 * (size_t)ni);
-        const uint4 b = ldg(nodes + 2 * (size_t)ni + 1);
+        uint4 a, b;
+        ldg_node(nodes + 2 * (size_t)ni, a, b);
         if (COUNT) k.nodes++;
         if (!box_hits(k.r, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), k.min_t, k.check_inside))
             continue;
@@ -290,8 +290,8 @@ PT_HD TraceResult traverse(const uint4* __restrict__ nodes, const float4* __rest
     while (sp > 0) {
         const uint32_t ni = stack[--sp];
         if (ni >= num_nodes) { res.overflow = true; break; }  // malformed tree guard
-        const uint4 a = ldg(nodes + 2 * (size_t)ni);
-        const uint4 b = ldg(nodes + 2 * (size_t)ni + 1);
+        uint4 a, b;
+        ldg_node(nodes + 2 * (size_t)ni, a, b);
         if (COUNT) res.nodes++;
         if (!box_hits(r, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w),
                       bitsf(b.x), bitsf(b.y), min_t, check_inside))
