@@ -128,6 +128,7 @@ struct pt_server {
     std::deque<Request*> pending;
     std::vector<Request*> active;     // admission order
     std::unordered_map<uint64_t, std::unique_ptr<Request>> all;
+    std::vector<std::unique_ptr<Request>> failed;  // fetched failures, freed at destroy
     bool stop = false;
     bool blocked = false;             // admission waits for device or host memory to free up
     uint64_t next_ticket = 1;
@@ -567,27 +568,39 @@ extern "C" int pt_server_wait(pt_server* s, uint64_t ticket, uint32_t timeout_ms
 
 extern "C" int pt_server_fetch(pt_server* s, uint64_t ticket, float* rgb_out, uint32_t* primary_out) {
     if (!s) return fail(PT_EINVAL, "server is NULL");
-    std::unique_lock<std::mutex> lock(s->mu);
-    auto it = s->all.find(ticket);
-    if (it == s->all.end()) return fail(PT_EINVAL, "unknown ticket");
-    Request* r = it->second.get();
-    if (r->state != 2 && r->state >= 0) return fail(PT_EINVAL, "request not finished");
-    const int st = r->state;
+    std::unique_ptr<Request> r;
+    std::string err;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        auto it = s->all.find(ticket);
+        if (it == s->all.end()) return fail(PT_EINVAL, "unknown ticket");
+        if (it->second->state != 2 && it->second->state >= 0) return fail(PT_EINVAL, "request not finished");
+        r = std::move(it->second);  // the ticket is gone; its arena block stays taken until released below
+        s->all.erase(it);
+        err = s->worker_error;
+    }
+    // copy out without the server lock, so the scheduler keeps planning while a large film is copied
     const size_t n = r->npix;
-    if (st == 2) {
+    if (r->state == 2) {
         const char* h = s->arena + r->host_off;
         if (rgb_out) std::memcpy(rgb_out, h, 12 * n);
         if (primary_out) std::memcpy(primary_out, h + 12 * n, 4 * n);
     }
-    if (r->host_off != ~(size_t)0) {
-        s->arena_alloc.release(r->host_off, host_bytes(r->npix));
-        s->blocked = false;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (r->host_off != ~(size_t)0) {
+            s->arena_alloc.release(r->host_off, host_bytes(r->npix));
+            s->blocked = false;
+        }
+        if (r->state < 0) {
+            const int st = r->state;
+            // a failed request may still be named by a queued wave: keep it alive until destroy
+            s->failed.push_back(std::move(r));
+            s->cv.notify_one();
+            return fail(st, "request failed: " + err);
+        }
     }
-    s->all.erase(it);
-    const std::string err = s->worker_error;
-    lock.unlock();
     s->cv.notify_one();  // admission may have waited for arena space
-    if (st < 0) return fail(st, "request failed: " + err);
     return PT_OK;
 }
 
