@@ -316,14 +316,22 @@ class Scene:
     def intersect(self, rays, hits=None, device: bool = False, stream: int = 0, counts: bool = False):
         """Scene::intersect for a batch: numpy (host) arrays, or torch CUDA tensors with device=True
         (asynchronous on `stream`).  Returns hits (and node/face test counts with counts=True)."""
-        n = len(rays) if not hasattr(rays, "numel") else rays.numel() // 8
+        nbytes = lambda x: x.numel() * x.element_size() if hasattr(x, "numel") else x.nbytes
+        if device:
+            # counts come from byte sizes, so a tensor of any element type is read correctly
+            if nbytes(rays) % RAY_DTYPE.itemsize:
+                raise ValueError("device rays must be a whole number of 32-byte pt_ray records")
+            n = nbytes(rays) // RAY_DTYPE.itemsize
+        else:
+            rays = np.ascontiguousarray(rays, RAY_DTYPE)
+            n = len(rays)
         if hits is None:
             if device:
                 raise ValueError("device calls need a preallocated hits tensor")
             hits = np.zeros(n, HIT_DTYPE)
+        if nbytes(hits) < n * HIT_DTYPE.itemsize:
+            raise ValueError(f"hits buffer holds {nbytes(hits)} bytes, {n} hits need {n * HIT_DTYPE.itemsize}")
         flags = MEM_DEVICE if device else 0
-        if not device:
-            rays = np.ascontiguousarray(rays, RAY_DTYPE)
         if counts:
             if device:
                 raise ValueError("counts are host-only here")

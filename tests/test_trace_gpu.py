@@ -176,3 +176,24 @@ def test_reference_built_tree_passthrough(cuda_device):
     with pytest.raises(pb.PolytopeError) as e:
         pb.Scene(meshes, env, nodes=bad, leaf_pairs=pairs)
     assert e.value.code == pb.PT_EINVAL
+
+
+def test_device_intersect_takes_counts_from_byte_sizes(cuda_device):
+    """Device buffers of any element type: the ray count is bytes / 32, and a hits buffer too small
+    for it is refused before anything reaches the GPU."""
+    import torch
+    meshes, rays = W.microbench(n_rays=4096, level=4)
+    scene = pb.Scene(meshes)
+    exp = scene.intersect(rays)
+    as_bytes = torch.from_numpy(rays.view(np.uint8)).cuda()
+    as_float = torch.from_numpy(rays.view(np.float32)).cuda()
+    for dr in (as_bytes, as_float):
+        hits = torch.zeros(len(rays) * 16, dtype=torch.uint8, device="cuda")
+        scene.intersect(dr, hits, device=True)
+        torch.cuda.synchronize()
+        assert hits.cpu().numpy().tobytes() == exp.tobytes()
+    with pytest.raises(ValueError):
+        scene.intersect(as_bytes, torch.zeros(len(rays) * 16 - 1, dtype=torch.uint8, device="cuda"), device=True)
+    with pytest.raises(ValueError):
+        scene.intersect(as_bytes[:-4], torch.zeros(len(rays) * 16, dtype=torch.uint8, device="cuda"), device=True)
+
