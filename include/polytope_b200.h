@@ -166,7 +166,7 @@ int pt_trace_counted(pt_scene *scene, const pt_ray *rays, uint64_t n, pt_hit *hi
                      uint32_t *node_tests, uint32_t *tri_tests, uint32_t mem_flags, void *stream);
 
 /* Launch shape of the ray-query kernel (per scene).  shared_stack: traversal-stack entries per
- * lane kept in shared memory (0, 8 or 16; the rest stays in local memory); queue_chunk: rays a
+ * lane kept in shared memory (0, 8, 16, 24 or 32; the rest stays in local memory); queue_chunk: rays a
  * warp takes per fetch (multiple of 32).  Results do not depend on it. */
 typedef struct pt_trace_tuning {
     uint32_t shared_stack;
@@ -174,8 +174,8 @@ typedef struct pt_trace_tuning {
 } pt_trace_tuning;
 int pt_scene_set_trace_tuning(pt_scene *scene, const pt_trace_tuning *tuning);
 int pt_scene_get_trace_tuning(const pt_scene *scene, pt_trace_tuning *tuning);
-/* Times the candidate shapes on the given device rays (CUDA events, mean of three launches after
- * a warm-up, one knob at a time), keeps the fastest on the scene and returns it. */
+/* Times the candidate shapes on the given device rays (CUDA events, fastest of five launches
+ * after a warm-up, one knob at a time), keeps the fastest on the scene and returns it. */
 int pt_trace_autotune(pt_scene *scene, const pt_ray *rays_dev, uint64_t n, pt_hit *hits_dev,
                       pt_trace_tuning *best, float *best_ms);
 

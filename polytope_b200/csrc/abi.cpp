@@ -410,8 +410,8 @@ int pt_trace_counted(pt_scene* scene, const pt_ray* rays, uint64_t n, pt_hit* hi
 
 int pt_scene_set_trace_tuning(pt_scene* scene, const pt_trace_tuning* t) {
     if (!scene || !t) return fail(PT_EINVAL, "scene or tuning is NULL");
-    if (t->shared_stack != 0 && t->shared_stack != 8 && t->shared_stack != 16)
-        return fail(PT_EINVAL, "shared_stack must be 0, 8 or 16");
+    if (t->shared_stack > 32 || (t->shared_stack & 7u))
+        return fail(PT_EINVAL, "shared_stack must be 0, 8, 16, 24 or 32");
     if (t->queue_chunk < 32 || t->queue_chunk > 4096 || (t->queue_chunk & 31u))
         return fail(PT_EINVAL, "queue_chunk must be a multiple of 32 in [32, 4096]");
     scene->trace_tuning = *t;
@@ -437,17 +437,20 @@ int pt_trace_autotune(pt_scene* scene, const pt_ray* rays_dev, uint64_t n, pt_hi
         scene->trace_tuning = t;
         int rc = pt_trace(scene, rays_dev, n, hits_dev, PT_MEM_DEVICE, nullptr);  // warm-up
         if (rc) return rc;
-        cudaEventRecord(e0, 0);
-        for (int r = 0; r < 3; ++r)
+        ms = 1e30f;
+        for (int r = 0; r < 5; ++r) {  // fastest of five single launches: robust to a noisy neighbour
+            cudaEventRecord(e0, 0);
             if ((rc = pt_trace(scene, rays_dev, n, hits_dev, PT_MEM_DEVICE, nullptr))) return rc;
-        cudaEventRecord(e1, 0);
-        cudaEventSynchronize(e1);
-        cudaEventElapsedTime(&ms, e0, e1);
-        ms /= 3.f;
+            cudaEventRecord(e1, 0);
+            cudaEventSynchronize(e1);
+            float one = 0.f;
+            cudaEventElapsedTime(&one, e0, e1);
+            ms = std::min(ms, one);
+        }
         return PT_OK;
     };
     int rc = PT_OK;
-    for (uint32_t sh : {0u, 8u, 16u}) {
+    for (uint32_t sh : {0u, 8u, 16u, 24u, 32u}) {
         pt_trace_tuning t = cur;
         t.shared_stack = sh;
         float ms = 0.f;

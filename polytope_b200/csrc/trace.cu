@@ -122,8 +122,13 @@ cudaError_t launch_trace(const TraceArgs& a, cudaStream_t s) {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const bool counted = a.node_tests || a.tri_tests;
         const int sh = a.shared_stack;
-        auto kern_f = sh >= 16 ? trace_persistent_kernel<false, 16> : (sh >= 8 ? trace_persistent_kernel<false, 8> : trace_persistent_kernel<false, 0>);
-        auto kern_t = sh >= 16 ? trace_persistent_kernel<true, 16> : (sh >= 8 ? trace_persistent_kernel<true, 8> : trace_persistent_kernel<true, 0>);
+        auto pick = [sh](auto k0, auto k8, auto k16, auto k24, auto k32) {
+            return sh >= 32 ? k32 : sh >= 24 ? k24 : sh >= 16 ? k16 : sh >= 8 ? k8 : k0;
+        };
+        auto kern_f = pick(trace_persistent_kernel<false, 0>, trace_persistent_kernel<false, 8>, trace_persistent_kernel<false, 16>,
+                           trace_persistent_kernel<false, 24>, trace_persistent_kernel<false, 32>);
+        auto kern_t = pick(trace_persistent_kernel<true, 0>, trace_persistent_kernel<true, 8>, trace_persistent_kernel<true, 16>,
+                           trace_persistent_kernel<true, 24>, trace_persistent_kernel<true, 32>);
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, counted ? kern_t : kern_f, 128, 0);
         if (e != cudaSuccess) return e;
         if (per_sm < 1) per_sm = 1;
