@@ -343,8 +343,11 @@ typedef struct pt_server_config {
 
 typedef struct pt_server_stats {
     uint64_t waves, completed, rays_traced;
-    double   busy_ms;                 /* host-measured time the GPU spent on waves                */
+    double   busy_ms;                 /* GPU time of the waves (CUDA events)                       */
     uint64_t pending, active, device_bytes_in_use;
+    double   blocked_ms;              /* scheduler time with requests queued but no room to admit
+                                         them (in-flight limit, device budget or host arena)    */
+    uint64_t host_bytes_in_use;       /* host arena bytes held by finished, unfetched films      */
 } pt_server_stats;
 
 typedef struct pt_server pt_server;

@@ -156,7 +156,8 @@ struct pt_server {
     size_t table_bytes = 0;
     // statistics
     uint64_t waves = 0, completed = 0, rays_traced = 0;
-    double busy_ms = 0.0;
+    double busy_ms = 0.0, blocked_ms = 0.0;
+    size_t host_in_use = 0;
 
     void run();
     void admit();
@@ -212,6 +213,7 @@ void pt_server::admit() {
             continue;
         }
         r->host_off = off;
+        host_in_use += host_bytes(r->npix);
         r->bytes = need;
         mem_in_use += need;
         r->params.rays_traced = nullptr;
@@ -391,8 +393,12 @@ void pt_server::run() {
         bool stopping;
         {
             std::unique_lock<std::mutex> lock(mu);
-            if (queued.empty())
+            if (queued.empty()) {
+                const bool waiting_for_room = !pending.empty() && blocked;
+                const auto t0 = Clock::now();
                 cv.wait(lock, [&] { return stop || (!pending.empty() && !blocked) || has_unplanned(); });
+                if (waiting_for_room) blocked_ms += std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+            }
             stopping = stop;
             if (!stopping) {
                 admit();
@@ -590,6 +596,7 @@ extern "C" int pt_server_fetch(pt_server* s, uint64_t ticket, float* rgb_out, ui
         std::lock_guard<std::mutex> lock(s->mu);
         if (r->host_off != ~(size_t)0) {
             s->arena_alloc.release(r->host_off, host_bytes(r->npix));
+            s->host_in_use -= host_bytes(r->npix);
             s->blocked = false;
         }
         if (r->state < 0) {
@@ -614,6 +621,8 @@ extern "C" int pt_server_get_stats(pt_server* s, pt_server_stats* st) {
     st->pending = s->pending.size();
     st->active = s->active.size();
     st->device_bytes_in_use = s->mem_in_use;
+    st->blocked_ms = s->blocked_ms;
+    st->host_bytes_in_use = s->host_in_use;
     return PT_OK;
 }
 
