@@ -210,6 +210,13 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WfItem* __restrict_
 // stores the clamped radiance and takes the next slot.  Warps take slots in chunks of `chunk`
 // from *fetch and refill idle lanes from the chunk, so a warp no longer waits for its longest
 // path.  The first SH stack entries of a lane live in shared memory.
+//
+// Shading runs in batches: a lane whose ray has ended waits (idle) until at least kShadeBatch
+// lanes of its warp are in the same state, or no lane is still walking, and then those lanes shade
+// together, so the long shading code is not replayed by the warp for one or two lanes at a time.
+// Each lane's own sequence of operations is unchanged.
+constexpr int kShadeBatch = 16;
+
 template <int CAP, int SH>
 __global__ void __launch_bounds__(128, 5) wf_path_kernel(const WfItem* __restrict__ items, const WfSegment* __restrict__ segs,
                                                       uint32_t nseg, uint32_t count, float* __restrict__ radiance,
@@ -231,6 +238,7 @@ __global__ void __launch_bounds__(128, 5) wf_path_kernel(const WfItem* __restric
     const float4* tris = nullptr;
     PathState s;
     F3 contrib = f3(0.f, 0.f, 0.f);
+    bool finished = false, walk_ok = true;  // the current ray's walk has ended (and how)
     while (true) {
         const uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
         if (need && !exhausted && pool_next >= pool_end) {
@@ -264,6 +272,7 @@ __global__ void __launch_bounds__(128, 5) wf_path_kernel(const WfItem* __restric
                 shadow = false;
                 walk_begin(k, s.o.x, s.o.y, s.o.z, s.d.x, s.d.y, s.d.z, inf, false);
                 active = true;
+                finished = false;
             }
             const uint64_t took = (uint64_t)__popc(need) < avail ? (uint64_t)__popc(need) : avail;
             pool_next += took;
@@ -272,11 +281,21 @@ __global__ void __launch_bounds__(128, 5) wf_path_kernel(const WfItem* __restric
             if (exhausted) break;
             continue;
         }
-        if (active) {
+        if (active && !finished) {
             uint32_t leaf_off = 0, leaf_n = 0;
             const bool ok = walk_to_leaf<false>(k, nodes, num_nodes, leaf_off, leaf_n);
             if (ok && leaf_n) walk_leaf<false>(k, tris, leaf_off, leaf_n);
             if (!ok || k.done || k.sp == 0) {
+                finished = true;
+                walk_ok = ok;
+            }
+        }
+        const uint32_t fin = __ballot_sync(0xFFFFFFFFu, active && finished);
+        const uint32_t walking = __ballot_sync(0xFFFFFFFFu, active && !finished);
+        if (fin && (walking == 0 || __popc(fin) >= kShadeBatch)) {
+            if (active && finished) {
+                finished = false;
+                const bool ok = walk_ok;
                 ++rays;
                 bool go = false;
                 if (!ok) {
