@@ -568,12 +568,14 @@ def main():
             "t_error_vs_fp64": t_err,
             "step_ms": {"min": round(min(per), 4), "median": round(statistics.median(per), 4), "max": round(max(per), 4)},
         }
+        # the serving measurement is host-clocked (arrivals, latencies), so it runs first, before
+        # the batched and full-frame sections have churned the device and host memory
+        if not args.no_served and world == 1:
+            line["served"] = bench_served(pb, torch)
         if not args.no_batched and world == 1:
             line["batched"] = bench_batched(pb, torch)
         if not args.no_render and world == 1:
             line["render"] = bench_render(pb, torch, cpu=not args.no_cpu_baseline)
-        if not args.no_served and world == 1:
-            line["served"] = bench_served(pb, torch)
         if not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             v, kind, dt = cpu_reference(meshes, rays, args.ref_sample, threads)
