@@ -333,7 +333,8 @@ int pt_batch_autotune(const pt_batch_item *items, uint32_t n, pt_batch_tuning *b
 
 typedef struct pt_server_config {
     uint32_t        max_inflight;     /* requests admitted at once                                 */
-    uint64_t        memory_budget;    /* device bytes for admitted requests' films (0 = 80 % free) */
+    uint64_t        memory_budget;    /* device bytes for admitted requests' films (0 = 80 % of
+                                         the memory free when the server is created)             */
     uint64_t        wave_pixels;      /* work per wave: pixels (PT_PIPELINE_FUSED) or paths (others) */
     pt_batch_tuning tuning;
     uint32_t        policy;           /* PT_SERVE_OLDEST_FIRST or PT_SERVE_FAIR_SHARE              */
@@ -348,6 +349,9 @@ typedef struct pt_server_stats {
     double   blocked_ms;              /* scheduler time with requests queued but no room to admit
                                          them (in-flight limit, device budget or host arena)    */
     uint64_t host_bytes_in_use;       /* host arena bytes held by finished, unfetched films      */
+    double   plan_ms;                 /* scheduler time admitting, planning and enqueueing waves  */
+    double   retire_wait_ms;          /* scheduler time waiting for waves and their film copies   */
+    uint64_t waves_launched;          /* waves enqueued (waves counts retired ones)               */
 } pt_server_stats;
 
 typedef struct pt_server pt_server;

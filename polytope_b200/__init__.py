@@ -127,7 +127,8 @@ class RequestTiming(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("waves", C.c_uint64), ("completed", C.c_uint64), ("rays_traced", C.c_uint64), ("busy_ms", C.c_double),
                 ("pending", C.c_uint64), ("active", C.c_uint64), ("device_bytes_in_use", C.c_uint64),
-                ("blocked_ms", C.c_double), ("host_bytes_in_use", C.c_uint64)]
+                ("blocked_ms", C.c_double), ("host_bytes_in_use", C.c_uint64), ("plan_ms", C.c_double),
+                ("retire_wait_ms", C.c_double), ("waves_launched", C.c_uint64)]
 
 
 def _load() -> C.CDLL:

@@ -54,6 +54,7 @@ struct Request {
     size_t bytes = 0;             // device bytes
     void* dev = nullptr;          // RenderParams, rgb (3 floats/px), primary ids, film sums (wave pipelines)
     size_t host_off = ~(size_t)0; // finished film in the host arena: rgb then primary ids
+    uint32_t param_slot = ~0u;    // pinned staging slot of its parameters while admitted
     int state = 0;                // 0 queued, 1 admitted, 2 done, < 0 error
     bool launched = false, retired = false;
     Clock::time_point submitted, admitted, first_wave, last_wave, done;
@@ -139,6 +140,11 @@ struct pt_server {
     cudaStream_t copy_stream = nullptr;  // finished films -> host arena
     cudaMemPool_t pool = nullptr;        // request memory (stream-ordered)
     cudaEvent_t ev_start[kWavesQueued] = {}, ev_end[kWavesQueued] = {}, ev_copied[kWavesQueued] = {};
+    // Pinned staging of each admitted request's parameters: a copy from pageable memory would
+    // first wait for everything already queued on the stream, stalling the scheduler behind the
+    // running waves.  One 256-byte slot per in-flight request.
+    char* h_params = nullptr;
+    std::vector<uint32_t> free_param_slots;
     char* arena = nullptr;               // pinned host memory for finished films
     size_t arena_size = 0;
     ArenaAllocator arena_alloc;          // guarded by mu
@@ -156,7 +162,8 @@ struct pt_server {
     size_t table_bytes = 0;
     // statistics
     uint64_t waves = 0, completed = 0, rays_traced = 0;
-    double busy_ms = 0.0, blocked_ms = 0.0;
+    double busy_ms = 0.0, blocked_ms = 0.0, plan_ms = 0.0, retire_wait_ms = 0.0;
+    uint64_t waves_launched = 0;
     size_t host_in_use = 0;
 
     void run();
@@ -177,15 +184,7 @@ struct pt_server {
 // device, so a request larger than the budget still runs alone.
 void pt_server::admit() {
     if (pending.empty()) return;
-    size_t budget = cfg.memory_budget;
-    if (!budget) {
-        size_t free_b = 0, total_b = 0;
-        cudaMemGetInfo(&free_b, &total_b);
-        uint64_t reserved = 0, used = 0;
-        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
-        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
-        budget = (size_t)(0.8 * (double)(free_b + (reserved > used ? reserved - used : 0))) + mem_in_use;
-    }
+    const size_t budget = cfg.memory_budget;  // fixed at creation: a driver query per admission cost milliseconds
     blocked = false;
     while (!pending.empty() && active.size() < cfg.max_inflight) {
         Request* r = pending.front();
@@ -217,7 +216,11 @@ void pt_server::admit() {
         r->bytes = need;
         mem_in_use += need;
         r->params.rays_traced = nullptr;
-        cudaMemcpyAsync(r->dev, &r->params, sizeof(r->params), cudaMemcpyHostToDevice, stream);
+        r->param_slot = free_param_slots.back();  // active.size() < max_inflight, so one is free
+        free_param_slots.pop_back();
+        char* hp = h_params + 256 * (size_t)r->param_slot;
+        std::memcpy(hp, &r->params, sizeof(r->params));
+        cudaMemcpyAsync(r->dev, hp, sizeof(r->params), cudaMemcpyHostToDevice, stream);
         if (wave_engine) cudaMemsetAsync(req_film(r), 0, 12 * (size_t)r->npix, stream);
         r->state = 1;
         r->admitted = Clock::now();
@@ -337,6 +340,10 @@ cudaError_t pt_server::enqueue(WaveInFlight& w, const std::vector<uint32_t>& tak
 // Returns a request's device memory to the pool, stream-ordered after its film copies, and drops
 // it from the active set (mu held).  Its film stays in the host arena until fetched.
 void pt_server::release_device(Request* r) {
+    if (r->param_slot != ~0u) {  // its copy ran long before the request's waves finished
+        free_param_slots.push_back(r->param_slot);
+        r->param_slot = ~0u;
+    }
     if (r->dev) {
         cudaFreeAsync(r->dev, copy_stream);
         r->dev = nullptr;
@@ -401,23 +408,32 @@ void pt_server::run() {
             }
             stopping = stop;
             if (!stopping) {
+                const auto t0 = Clock::now();
                 admit();
                 plan(w, take, first);
+                plan_ms += std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
             }
         }
         if (stopping && queued.empty()) return;
         const bool launched = !w.members.empty();
         if (launched) {
+            const auto t0 = Clock::now();
             w.slot = next_slot;
             next_slot = (next_slot + 1) % kWavesQueued;
             w.launch = enqueue(w, take, first);
             queued.push_back(std::move(w));
+            std::lock_guard<std::mutex> lock(mu);
+            plan_ms += std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+            ++waves_launched;
         }
         // Retire the oldest wave when the queue is full, or when there was nothing to launch
         // (its completion frees memory and in-flight slots for the next admissions).
         if (!queued.empty() && (queued.size() >= (size_t)kWavesQueued || !launched)) {
+            const auto t0 = Clock::now();
             retire(queued.front());
             queued.pop_front();
+            std::lock_guard<std::mutex> lock(mu);
+            retire_wait_ms += std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
         }
     }
 }
@@ -437,6 +453,7 @@ void destroy_resources(pt_server* s) {
     if (s->d_counters) cudaFree(s->d_counters);
     if (s->h_items) cudaFreeHost(s->h_items);
     if (s->h_rays) cudaFreeHost(s->h_rays);
+    if (s->h_params) cudaFreeHost(s->h_params);
     if (s->arena) cudaFreeHost(s->arena);
     if (s->d_wave) cudaFree(s->d_wave);
     if (s->d_tables) cudaFree(s->d_tables);
@@ -459,6 +476,11 @@ extern "C" int pt_server_create(const pt_server_config* cfg, pt_server** out) {
     if (!s->cfg.wave_pixels) s->cfg.wave_pixels = 1u << 20;
     s->arena_size = cfg->host_budget ? (size_t)up256(cfg->host_budget) : ((size_t)1 << 30);
     if (cudaGetDevice(&s->device) != cudaSuccess) return fail(PT_ECUDA, "no CUDA device available");
+    if (!s->cfg.memory_budget) {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return fail(PT_ECUDA, "cudaMemGetInfo failed");
+        s->cfg.memory_budget = (uint64_t)(0.8 * (double)free_b);
+    }
     s->max_items = std::min<uint32_t>(cfg->max_inflight, 4096);
     s->wave_engine = cfg->tuning.pipeline != PT_PIPELINE_FUSED;
     cudaMemPoolProps props{};
@@ -472,12 +494,14 @@ extern "C" int pt_server_create(const pt_server_config* cfg, pt_server** out) {
               cudaMallocHost((void**)&s->h_items, sizeof(BatchItem) * s->max_items * kWavesQueued) == cudaSuccess &&
               cudaMallocHost((void**)&s->h_rays, sizeof(unsigned long long) * kWavesQueued) == cudaSuccess &&
               cudaMallocHost((void**)&s->arena, s->arena_size) == cudaSuccess &&
+              cudaMallocHost((void**)&s->h_params, 256 * (size_t)cfg->max_inflight) == cudaSuccess &&
               cudaMalloc(&s->d_counters, 16) == cudaSuccess && cudaMemset(s->d_counters, 0, 16) == cudaSuccess;
     for (int i = 0; ok && i < kWavesQueued; ++i)
         ok = cudaEventCreate(&s->ev_start[i]) == cudaSuccess && cudaEventCreate(&s->ev_end[i]) == cudaSuccess &&
              cudaEventCreateWithFlags(&s->ev_copied[i], cudaEventDisableTiming) == cudaSuccess;
     if (ok) {
         s->arena_alloc.reset(s->arena_size);
+        for (uint32_t i = cfg->max_inflight; i-- > 0;) s->free_param_slots.push_back(i);
         // keep freed request memory in the pool for the next admissions instead of returning it
         // to the driver at every synchronisation
         uint64_t keep = ~0ull;
@@ -623,6 +647,9 @@ extern "C" int pt_server_get_stats(pt_server* s, pt_server_stats* st) {
     st->device_bytes_in_use = s->mem_in_use;
     st->blocked_ms = s->blocked_ms;
     st->host_bytes_in_use = s->host_in_use;
+    st->plan_ms = s->plan_ms;
+    st->retire_wait_ms = s->retire_wait_ms;
+    st->waves_launched = s->waves_launched;
     return PT_OK;
 }
 
