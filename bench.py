@@ -314,7 +314,7 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
                      "films by DMA into a 2 GiB pinned arena; a client thread copies results out in submission order "
                      "into reused buffers (the plain arm renders into the same reused buffers)",
            "timing": "host steady clock from the first arrival to the last completion (film in host memory); latency = completion - arrival; "
-                     "each arm's run with the median makespan of 3 (runs: [Mrays/s, p99 ms] of each)",
+                     "each arm's run with the median makespan of 3 (runs: [Mrays/s, p99 ms(, GPU busy ms of the waves)] of each)",
            "rates": []}
     def summary(lat, span, rays):
         return {"mrays_s": round(rays / span / 1e6, 1), "p50_ms": pct(lat, 50), "p95_ms": pct(lat, 95),
@@ -326,8 +326,12 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
         arrivals = unit / rate
         served, plain = [], []
         for _ in range(repeats):
+            s0 = srv.stats()
             lat_s, span_s, rays = run_served(pb, srv, scenes, reqs, arrivals, films)
+            s1 = srv.stats()
             served.append(summary(lat_s, span_s, rays))
+            served[-1]["gpu_busy_ms"] = round(s1["busy_ms"] - s0["busy_ms"], 1)
+            served[-1]["waves"] = int(s1["waves"] - s0["waves"])
             lat_p, span_p = run_plain(pb, scenes, reqs, arrivals, films)
             plain.append(summary(lat_p, span_p, rays))
         med = lambda runs: sorted(runs, key=lambda r: r["makespan_s"])[len(runs) // 2]
@@ -335,7 +339,7 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
         out["rates"].append({
             "rate_per_s": rate,
             "served": med(served), "plain_per_request": med(plain),
-            "runs": {"served": [(r["mrays_s"], r["p99_ms"]) for r in served],
+            "runs": {"served": [(r["mrays_s"], r["p99_ms"], r["gpu_busy_ms"]) for r in served],
                      "plain_per_request": [(r["mrays_s"], r["p99_ms"]) for r in plain]}})
     srv.close()
     return out
