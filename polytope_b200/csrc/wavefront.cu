@@ -218,7 +218,7 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WfItem* __restrict_
 constexpr int kShadeBatch = 16;
 
 template <int CAP, int SH>
-__global__ void __launch_bounds__(128, 5) wf_path_kernel(const WfItem* __restrict__ items, const WfSegment* __restrict__ segs,
+__global__ void __launch_bounds__(128, 7) wf_path_kernel(const WfItem* __restrict__ items, const WfSegment* __restrict__ segs,
                                                       uint32_t nseg, uint32_t count, float* __restrict__ radiance,
                                                       unsigned long long* fetch, uint32_t chunk,
                                                       unsigned long long* rays_traced) {
