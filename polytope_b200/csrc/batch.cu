@@ -432,9 +432,9 @@ extern "C" int pt_batch_autotune(const pt_batch_item* items, uint32_t n, pt_batc
         if (knob == 3) for (uint32_t v : {24u, 32u, 48u, 64u}) { if (v < max_depth + 2) continue; auto c = cur; c.stack_depth = v; cands.push_back(c); }
         if (knob == 4) {
             const uint64_t limit = cur.pipeline == PT_PIPELINE_FUSED ? total : total_paths;
-            const uint64_t opts_f[] = {0ull, 1ull << 20, 1ull << 22};
-            const uint64_t opts_w[] = {1ull << 20, 1ull << 22, 1ull << 23};
-            for (int k = 0; k < 3; ++k) {
+            const uint64_t opts_f[] = {0ull, 1ull << 20, 1ull << 22, 1ull << 24};
+            const uint64_t opts_w[] = {1ull << 22, 1ull << 23, 1ull << 24, 1ull << 25};  // larger waves: shorter tails
+            for (int k = 0; k < 4; ++k) {
                 const uint64_t v = cur.pipeline == PT_PIPELINE_FUSED ? opts_f[k] : opts_w[k];
                 if (v && v >= limit) continue;
                 auto c = cur;
