@@ -96,6 +96,8 @@ def test_server_results_same_alone_and_in_the_mix(cuda_device, pipeline, policy)
         assert_bit_equal(rgb, solo(scene, rd)[0], "server vs pt_render")
     s = srv.stats()
     assert s["completed"] == 24 and s["waves"] >= 12 and s["rays_traced"] > 0 and s["device_bytes_in_use"] == 0
+    assert s["host_bytes_in_use"] == 0 and s["waves_launched"] == s["waves"] and s["busy_ms"] > 0
+    assert s["plan_ms"] >= 0 and s["retire_wait_ms"] >= 0 and s["blocked_ms"] >= 0
     srv.close()
 
 
