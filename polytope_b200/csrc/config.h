@@ -4,3 +4,22 @@
 // Traversal stack entries per ray.  The reference's ordered DFS needs at most (tree depth + 1)
 // entries; pt_scene_create records the depth and calls refuse trees that do not fit.
 #define PT_TRAVERSAL_STACK 64
+
+// Warp rounds of the persistent walks (walk_round, traverse.cuh): the lanes of a warp take node
+// steps together until this many of them hold a leaf or have ended their walk (32 = every walking
+// lane), then test faces together; 0 walks each lane on its own to its next leaf instead (no vote,
+// fewer live registers).  One value per kernel: the ray-query kernel, the persistent path kernel
+// and the wavefront extend/shadow kernel.  Measured on a B200 (each against the per-lane walk):
+// ray queries on the 1.3 M-face microbench 1722 -> 1985 Mrays/s at 16 (12: 1937, 24: slower);
+// whole paths on the 6.5 M-face frame 1595 -> 1678 Msamples/s at 12 (8 and 16 slower); the
+// wavefront kernel, held to 64 registers, lost 17 % to the vote's extra live state, so it walks
+// per lane.
+#ifndef PT_LEAF_BATCH_TRACE
+#define PT_LEAF_BATCH_TRACE 16
+#endif
+#ifndef PT_LEAF_BATCH_PATHS
+#define PT_LEAF_BATCH_PATHS 12
+#endif
+#ifndef PT_LEAF_BATCH_WAVEFRONT
+#define PT_LEAF_BATCH_WAVEFRONT 0
+#endif

@@ -41,9 +41,9 @@ __global__ void __launch_bounds__(128) trace_kernel(const uint4* __restrict__ no
 // Persistent variant: a grid sized to the SMs; each warp takes chunks of kChunk rays from a global
 // counter and refills a lane as soon as its ray finishes, so lanes stay busy despite rays of very
 // different cost (any-hit rays stop early, closest-hit rays run long).  Each pass of the outer loop
-// runs every active lane's traversal to its next accepted leaf (while-while), then tests that
-// leaf's faces with the other lanes of the warp.  A ray's own node and face order is exactly the
-// reference's; only which rays share a warp changes.
+// steps the walking lanes node by node until PT_LEAF_BATCH_TRACE of them hold a leaf or have
+// ended, then tests those leaves' faces together (walk_round, traverse.cuh).  A ray's own node and face order is exactly
+// the reference's; only which rays share a warp, and when a lane waits, changes.
 template <bool COUNT, int SH>
 __global__ void __launch_bounds__(128, 9) trace_persistent_kernel(const uint4* __restrict__ nodes,
                                                                const float4* __restrict__ tris, uint32_t num_nodes,
@@ -92,10 +92,31 @@ __global__ void __launch_bounds__(128, 9) trace_persistent_kernel(const uint4* _
             }
             continue;
         }
+        uint32_t leaf_off = 0, leaf_n = 0;
+        bool ok, at_leaf;
+        if constexpr (PT_LEAF_BATCH_TRACE > 0) {
+            // walk_round (traverse.cuh), written out here: the compiler allocates this form with
+            // fewer spills, which measured 9 % faster on the 1.3 M-face microbench
+            ok = true;
+            at_leaf = false;
+            const uint32_t cand = __ballot_sync(0xFFFFFFFFu, active && k.sp > 0);
+            const int want = __popc(cand) < PT_LEAF_BATCH_TRACE ? __popc(cand) : PT_LEAF_BATCH_TRACE;
+            while (true) {
+                const bool walking = active && ok && !at_leaf && k.sp > 0;
+                const uint32_t w = __ballot_sync(0xFFFFFFFFu, walking);
+                if (w == 0 || __popc(cand & ~w) >= want) break;
+                if (walking) {
+                    const int r = walk_step<COUNT>(k, nodes, num_nodes, leaf_off, leaf_n);
+                    at_leaf = r > 0;
+                    ok = r >= 0;
+                }
+            }
+        } else {
+            ok = !active || walk_to_leaf<COUNT>(k, nodes, num_nodes, leaf_off, leaf_n);
+            at_leaf = active && ok && leaf_n > 0;
+        }
+        if (at_leaf) walk_leaf<COUNT>(k, tris, leaf_off, leaf_n);
         if (active) {
-            uint32_t leaf_off = 0, leaf_n = 0;
-            bool ok = walk_to_leaf<COUNT>(k, nodes, num_nodes, leaf_off, leaf_n);
-            if (ok && leaf_n) walk_leaf<COUNT>(k, tris, leaf_off, leaf_n);
             if (!ok || k.done || k.sp == 0) {
                 uint4 h;
                 h.x = ok ? k.prim : 0xFFFFFFFEu;

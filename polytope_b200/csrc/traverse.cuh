@@ -211,8 +211,38 @@ PT_HD void walk_begin(RayWalkT<CAP, SH>& k, float ox, float oy, float oz, float 
     k.stack.put(0, 0u);
 }
 
+// One step of the same walk: pops one node and tests its box.  Returns 1 when it is a leaf whose
+// box is hit (its faces in leaf_off / leaf_n), 0 for any other node, -1 on a guard failure.  The
+// caller checks k.sp > 0 first.  The persistent kernels step their lanes one node at a time with
+// it (walk_round) instead of walking each lane to its next leaf.
+template <bool COUNT, int CAP, int SH>
+PT_HD int walk_step(RayWalkT<CAP, SH>& k, const uint4* __restrict__ nodes, uint32_t num_nodes, uint32_t& leaf_off,
+                    uint32_t& leaf_n) {
+    const uint32_t ni = k.stack.get(--k.sp);
+    if (ni >= num_nodes) return -1;
+    uint4 a, b;
+    ldg_node(nodes + 2 * (size_t)ni, a, b);
+    if (COUNT) k.nodes++;
+    if (!box_hits(k.r, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), k.min_t, k.check_inside))
+        return 0;
+    const uint32_t nf = b.w & 0xFFFFu;
+    if (nf > 0) {
+        leaf_off = b.z;
+        leaf_n = nf;
+        return 1;
+    }
+    if (k.sp + 2 > CAP) return -1;
+    const uint32_t axis = b.w >> 16;
+    const bool neg = (axis == 0 ? k.r.ix : (axis == 1 ? k.r.iy : k.r.iz)) < 0;
+    const uint32_t hi = ni + b.z, lo = ni + 1;
+    k.stack.put(k.sp++, neg ? lo : hi);
+    k.stack.put(k.sp++, neg ? hi : lo);
+    return 0;
+}
+
 // Pops nodes in the reference order until a leaf whose box is hit comes up (returned in
-// leaf_off / leaf_n) or the stack runs empty.  Returns false on a guard failure.
+// leaf_off / leaf_n) or the stack runs empty.  Returns false on a guard failure.  The same
+// steps as walk_step, in one loop with the direction signs hoisted.
 template <bool COUNT, int CAP, int SH>
 PT_HD bool walk_to_leaf(RayWalkT<CAP, SH>& k, const uint4* __restrict__ nodes, uint32_t num_nodes, uint32_t& leaf_off,
                         uint32_t& leaf_n) {
@@ -241,6 +271,37 @@ PT_HD bool walk_to_leaf(RayWalkT<CAP, SH>& k, const uint4* __restrict__ nodes, u
     }
     return true;
 }
+
+// Warp-level schedule of walk_step (walk_round): the lanes of a warp that are walking take node
+// steps together until `batch` of them (or all, if fewer walk) have reached a leaf or ended their
+// walk; then those lanes test their leaves' faces together while the rest wait, and the rest
+// carry on walking in the next round.  A lane's own node and face sequence is the reference's
+// whatever the batch; the batch only decides how long a lane that found a leaf waits for others,
+// so that neither the node loop nor the face loop runs with a handful of lanes (stepping every
+// lane to its own next leaf left about 9 of 32 lanes busy on the 1.3 M-face microbench).
+// `walking` is this lane's eligibility at the start of the round; returns whether the lane walks
+// on, and sets at_leaf (faces to test in leaf_off / leaf_n) or ok = false (guard failure).
+#ifdef __CUDACC__
+template <bool COUNT, int CAP, int SH>
+__device__ __forceinline__ void walk_round(RayWalkT<CAP, SH>& k, bool walking, int batch, const uint4* __restrict__ nodes,
+                                           uint32_t num_nodes, bool& at_leaf, bool& ok, uint32_t& leaf_off,
+                                           uint32_t& leaf_n) {
+    at_leaf = false;
+    ok = true;
+    const uint32_t cand = __ballot_sync(0xFFFFFFFFu, walking);
+    const int want = __popc(cand) < batch ? __popc(cand) : batch;
+    while (true) {
+        const bool w_now = walking && ok && !at_leaf && k.sp > 0;
+        const uint32_t w = __ballot_sync(0xFFFFFFFFu, w_now);
+        if (w == 0 || __popc(cand & ~w) >= want) break;
+        if (w_now) {
+            const int r = walk_step<COUNT>(k, nodes, num_nodes, leaf_off, leaf_n);
+            at_leaf = r > 0;
+            ok = r >= 0;
+        }
+    }
+}
+#endif
 
 // The faces of one leaf in leaf order (Mesh::intersect per face, bvh.cpp:496-505).
 template <bool COUNT, int CAP, int SH>

@@ -138,10 +138,17 @@ __global__ void __launch_bounds__(256, kWfTraceMinBlocks) wf_trace_kernel(const 
             if (exhausted) break;
             continue;
         }
+        uint32_t leaf_off = 0, leaf_n = 0;
+        bool ok, at_leaf;
+        if constexpr (PT_LEAF_BATCH_WAVEFRONT > 0) {
+            walk_round<false>(k, active && k.sp > 0, PT_LEAF_BATCH_WAVEFRONT, nodes, num_nodes, at_leaf, ok, leaf_off,
+                              leaf_n);
+        } else {
+            ok = !active || walk_to_leaf<false, CAP>(k, nodes, num_nodes, leaf_off, leaf_n);
+            at_leaf = active && ok && leaf_n > 0;
+        }
+        if (at_leaf) walk_leaf<false, CAP>(k, tris, leaf_off, leaf_n);
         if (active) {
-            uint32_t leaf_off = 0, leaf_n = 0;
-            const bool ok = walk_to_leaf<false, CAP>(k, nodes, num_nodes, leaf_off, leaf_n);
-            if (ok && leaf_n) walk_leaf<false, CAP>(k, tris, leaf_off, leaf_n);
             if (!ok || k.done || k.sp == 0) {
                 if (!ok) atomicExch(err, 1);
                 if (SHADOW) {
@@ -215,8 +222,9 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WfItem* __restrict_
 
 // Whole paths of several renders in one persistent launch.  Each lane runs one path at a time
 // (the fused loop of path.cuh, with the same device functions in the same order, so results are
-// bit-identical): its current ray, closest-hit or shadow, is walked leaf by leaf (walk_to_leaf /
-// walk_leaf, while-while), and when it ends the lane shades, starts the path's next ray, or
+// bit-identical): its current ray, closest-hit or shadow, is walked node by node in warp rounds
+// (walk_round: PT_LEAF_BATCH_PATHS lanes at a leaf, then walk_leaf), and when it ends the lane
+// shades, starts the path's next ray, or
 // stores the clamped radiance and takes the next slot.  Warps take slots in chunks of `chunk`
 // from *fetch and refill idle lanes from the chunk, so a warp no longer waits for its longest
 // path.  The first SH stack entries of a lane live in shared memory.
@@ -291,11 +299,19 @@ __global__ void __launch_bounds__(128, 7) wf_path_kernel(const WfItem* __restric
             if (exhausted) break;
             continue;
         }
-        if (active && !finished) {
+        {
             uint32_t leaf_off = 0, leaf_n = 0;
-            const bool ok = walk_to_leaf<false>(k, nodes, num_nodes, leaf_off, leaf_n);
-            if (ok && leaf_n) walk_leaf<false>(k, tris, leaf_off, leaf_n);
-            if (!ok || k.done || k.sp == 0) {
+            bool ok, at_leaf;
+            if constexpr (PT_LEAF_BATCH_PATHS > 0) {
+                walk_round<false>(k, active && !finished && k.sp > 0, PT_LEAF_BATCH_PATHS, nodes, num_nodes, at_leaf, ok,
+                                  leaf_off, leaf_n);
+            } else {
+                const bool walking = active && !finished;
+                ok = !walking || walk_to_leaf<false>(k, nodes, num_nodes, leaf_off, leaf_n);
+                at_leaf = walking && ok && leaf_n > 0;
+            }
+            if (at_leaf) walk_leaf<false>(k, tris, leaf_off, leaf_n);
+            if (active && !finished && (!ok || k.done || k.sp == 0)) {
                 finished = true;
                 walk_ok = ok;
             }

@@ -55,6 +55,22 @@ def test_small_scene_full_config_matches_oracle(cuda_device, pipeline):
 
 
 @pytest.mark.parametrize("pipeline", PIPELINES, ids=["fused", "wavefront", "persistent"])
+def test_coincident_faces_render_matches_oracle(cuda_device, pipeline):
+    """The small scene with every sphere face listed twice (the copy's vertices rotated), so that
+    MinT rises on many camera, bounce and shadow rays; the film must still equal the oracle's."""
+    import dataclasses
+    meshes, env = W.small_scene(level=3)
+    sph = meshes[1]
+    meshes[1] = dataclasses.replace(sph, faces=np.concatenate([sph.faces, sph.faces[:, [1, 2, 0]]]))
+    scene = pb.Scene(meshes, env)
+    rgb, prim = pb.render(scene, 96, 72, 4, 4, W.SMALL_CAMERA, seed=3, flags=pb.RENDER_NEE | pipeline)
+    orgb, oprim = po.OracleScene(meshes, env).render(
+        dict(width=96, height=72, spp=4, max_depth=4, seed=3, camera=W.SMALL_CAMERA, flags=1))
+    assert_bit_equal(prim, oprim, "primary ids")
+    assert_bit_equal(rgb, orgb, "film")
+
+
+@pytest.mark.parametrize("pipeline", PIPELINES, ids=["fused", "wavefront", "persistent"])
 def test_instanced_scene_matches_reference_fixture(cuda_device, pipeline):
     g = load_golden("instanced_small.npz")
     im, env = W.instanced_scene(level=4)

@@ -197,3 +197,36 @@ def test_device_intersect_takes_counts_from_byte_sizes(cuda_device):
     with pytest.raises(ValueError):
         scene.intersect(as_bytes[:-4], torch.zeros(len(rays) * 16, dtype=torch.uint8, device="cuda"), device=True)
 
+
+
+def test_coincident_faces_that_raise_min_t(cuda_device):
+    """Every face twice, the copy with its vertices rotated: the copy's Wald t can round one ulp
+    above the running MinT and still be accepted (the range check compares T with MinT * det
+    before the division), so MinT rises during the walk and ties are decided by rounding.  Hits
+    and per-ray test counts must still equal the oracle's.  Rays aim at face interiors, so most
+    meet such a pair."""
+    x, y, z, f = pb.icosphere(4, 1.0, 0.05, 7)
+    m = pb.Mesh(x, y, z, np.concatenate([f, f[:, [1, 2, 0]]]))
+    scene = pb.Scene([m])
+    rng = np.random.default_rng(9)
+    n = 100_000
+    fi = f[rng.integers(0, len(f), n)]
+    w = rng.dirichlet([1, 1, 1], n).astype(np.float32)
+    tgt = sum(w[:, k:k + 1] * np.stack([x[fi[:, k]], y[fi[:, k]], z[fi[:, k]]], 1) for k in range(3))
+    o = rng.normal(size=(n, 3))
+    o = 3 * o / np.linalg.norm(o, axis=1)[:, None]
+    d = tgt - o
+    rays = np.zeros(n, pb.RAY_DTYPE)
+    rays["org"] = o
+    rays["dir"] = d / np.linalg.norm(d, axis=1)[:, None]
+    rays["tmax"] = np.inf
+    rays["flags"][1::4] = 1
+    rays["tmax"][1::4] = 3.5
+    hits, nt, tt = scene.intersect(rays, counts=True)
+    oh, ont, ott = po.OracleScene([m]).trace(rays, counts=True)
+    for fld in ("prim", "t", "u", "v"):
+        assert_bit_equal(hits[fld], oh[fld], fld)
+    assert_bit_equal(nt, ont, "nodes")
+    assert_bit_equal(tt, ott, "tris")
+    plain = scene.intersect(rays)
+    assert plain.tobytes() == hits.tobytes()
