@@ -235,8 +235,10 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WfItem* __restrict_
 // Each lane's own sequence of operations is unchanged.
 constexpr int kShadeBatch = 16;
 
+// 8 blocks of 128 per SM (64 registers, the rest spilled) measured fastest with the warp-voted
+// walk on the 6.5 M-face frame: 1700 Msamples/s against 1668 at 7 blocks, 1651 at 6, 1637 at 9.
 template <int CAP, int SH>
-__global__ void __launch_bounds__(128, 7) wf_path_kernel(const WfItem* __restrict__ items, const WfSegment* __restrict__ segs,
+__global__ void __launch_bounds__(128, 8) wf_path_kernel(const WfItem* __restrict__ items, const WfSegment* __restrict__ segs,
                                                       uint32_t nseg, uint32_t count, float* __restrict__ radiance,
                                                       unsigned long long* fetch, uint32_t chunk,
                                                       unsigned long long* rays_traced) {
