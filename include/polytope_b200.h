@@ -253,6 +253,37 @@ typedef struct pt_mesh_data {
 int pt_load_ply(const char *path, pt_mesh_data *out);
 void pt_mesh_data_free(pt_mesh_data *mesh);
 
+/* poly::pbrt_parser::parse_file (src/common/parsers/pbrt_parser.cpp:284-1711): a PBRT scene file
+ * read into the descriptions pt_scene_create and pt_render take.  Meshes come in the reference's
+ * poly::Scene::Shapes order with the transforms, materials and radiances the reference ends up
+ * with (including its in-place updates of a scope's transform and area light, the x255 radiance
+ * scale, the UV sphere tessellation of Shape "sphere" and ObjectBegin / ObjectInstance); plymesh
+ * paths are relative to the scene file.  Defaults as the reference's: 640x360, 8 samples, depth 5,
+ * field of view 90.  Supported: Sampler, Film "image", PixelFilter, Camera "perspective" set by at
+ * most one LookAt (none: the identity camera, returned as LookAt (0,0,0) (0,0,1) (0,1,0), the same
+ * matrix), Integrator "path", AttributeBegin/End, TransformBegin/End, Translate, Scale, Rotate,
+ * Transform, Material "matte" / "mirror", MakeNamedMaterial / NamedMaterial, AreaLightSource
+ * "diffuse", LightSource "infinite", Shape "plymesh" / "sphere", ObjectBegin / ObjectEnd /
+ * ObjectInstance.  Textures, Material "plastic", Shape "objmesh" and other camera transforms are
+ * rejected with PT_EINVAL and the reason; like the reference, other unknown directives are skipped.
+ * A shape with neither a material nor an area light comes back with material 0, which
+ * pt_scene_create rejects.  The mesh descriptions point into arrays owned by the handle
+ * (instances share them) and stay valid until pt_pbrt_free. */
+typedef struct pt_pbrt_scene pt_pbrt_scene;
+typedef struct pt_pbrt_info {
+    uint32_t  num_meshes;
+    int32_t   has_env;          /* LightSource "infinite" seen; env = its L x 255               */
+    float     env[3];
+    uint32_t  width, height;    /* Film "image" xresolution / yresolution                       */
+    uint32_t  spp;              /* Sampler pixelsamples                                          */
+    uint32_t  max_depth;        /* Integrator "path" maxdepth                                    */
+    pt_camera camera;           /* LookAt eye / look-at / up, Camera "perspective" fov           */
+} pt_pbrt_info;
+int pt_load_pbrt(const char *path, pt_pbrt_scene **out);
+int pt_pbrt_get_info(const pt_pbrt_scene *scene, pt_pbrt_info *info);
+int pt_pbrt_get_meshes(const pt_pbrt_scene *scene, const pt_mesh_desc **meshes);
+void pt_pbrt_free(pt_pbrt_scene *scene);
+
 /* ---- output format ------------------------------------------------------------------------ */
 
 /* The film as the reference's PNG output stores it: RGBA8, row-major, each channel

@@ -336,3 +336,39 @@ def ref_load_ply(path: str):
     f(str(path).encode(), C.byref(nv), C.byref(nf), C.byref(hn), *[v.ctypes.data for v in a + fv])
     normals = np.stack(a[3:], 1) if hn.value else None
     return a[0], a[1], a[2], np.stack(fv, 1), normals
+
+
+def ref_load_pbrt(path: str) -> dict:
+    """The reference's own pbrt_parser::parse_file (oracle/_ref) on a well-formed file: render
+    settings, camera and, per shape, geometry, transforms, material and radiance."""
+    lib = ref_lib()
+    lib.ref_pbrt_load.restype = C.c_void_p
+    lib.ref_pbrt_load.argtypes = [C.c_char_p]
+    lib.ref_pbrt_free.argtypes = [C.c_void_p]
+    lib.ref_pbrt_info.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.ref_pbrt_mesh.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p] + [C.c_void_p] * 9
+    h = lib.ref_pbrt_load(str(path).encode())
+    try:
+        u = np.zeros(6, np.uint32)
+        f = np.zeros(29, np.float32)
+        lib.ref_pbrt_info(h, u.ctypes.data, f.ctypes.data)
+        out = dict(width=int(u[0]), height=int(u[1]), spp=int(u[2]), max_depth=int(u[3]),
+                   env=tuple(f[0:3]) if u[5] else None, eye=f[3:6].copy(), look_at=f[6:9].copy(), up=f[9:12].copy(),
+                   fov=float(f[12]), camera_to_world=f[13:29].reshape(4, 4).copy(), meshes=[])
+        for i in range(int(u[4])):
+            mu = np.zeros(5, np.uint32)
+            mf = np.zeros(38, np.float32)
+            lib.ref_pbrt_mesh(h, i, mu.ctypes.data, mf.ctypes.data, *([None] * 9))
+            nv, nf = int(mu[0]), int(mu[1])
+            a = [np.zeros(nv, np.float32) for _ in range(6)]
+            fv = [np.zeros(nf, np.uint32) for _ in range(3)]
+            lib.ref_pbrt_mesh(h, i, mu.ctypes.data, mf.ctypes.data, *[v.ctypes.data for v in a + fv])
+            out["meshes"].append(dict(x=a[0], y=a[1], z=a[2], faces=np.stack(fv, 1) if nf else np.zeros((0, 3), np.uint32),
+                                      normals=np.stack(a[3:], 1) if mu[2] else None, material=int(mu[3]),
+                                      is_light=bool(mu[4]), object_to_world=mf[0:16].reshape(4, 4).copy(),
+                                      world_to_object=mf[16:32].reshape(4, 4).copy(), albedo=mf[32:35].copy(),
+                                      emission=mf[35:38].copy()))
+        return out
+    finally:
+        lib.ref_pbrt_free(h)
+

@@ -30,7 +30,11 @@
 #include <vector>
 
 #include "common/parsers/mesh_parsers.h"
+#include "common/parsers/pbrt_parser.h"
 #include "cpu/acceleration/bvh.h"
+#include "cpu/runners/AbstractRunner.h"
+#include "cpu/scenes/skyboxes/ColorSkybox.h"
+#include "cpu/shading/brdf/lambert_brdf.h"
 #include "cpu/cameras/PerspectiveCamera.h"
 #include "cpu/shading/brdf/mirror_brdf.h"
 #include "cpu/structures/stats.h"
@@ -57,10 +61,8 @@ void Logger::info(const std::string&) {}
 void Logger::warning(const std::string&) {}
 void Logger::error(const std::string& text) { std::fprintf(stderr, "%s\n", text.c_str()); }
 }  // namespace poly
-// Path globals of src/common/utilities/GlobalDefines.h (a header the reference's main.cpp
-// includes once); the parsers below only see absolute paths.
-std::string UnixPathSeparator = "/";
-std::string GetCurrentWorkingDirectory() { return std::string("/"); }
+// The path globals of src/common/utilities/GlobalDefines.h come from PNGFilm.cpp, which includes
+// that header; the parsers below only see absolute paths.
 thread_local poly::stats thread_stats;
 poly::stats main_stats;
 
@@ -535,6 +537,89 @@ int ref_load_ply(const char* path, uint32_t* num_vertices, uint32_t* num_faces, 
         }
     }
     return 0;
+}
+
+// ---- the reference's PBRT scene parser (pbrt_parser.cpp), for the pt_load_pbrt parity tests ----
+// ref_pbrt_load parses a file with poly::pbrt_parser::parse_file and keeps the runner it returns;
+// the accessors copy out what the renderer would use.  A file the reference cannot parse ends the
+// process (its ERROR macro exits), so the tests give it only well-formed files.
+
+struct RefPbrt {
+    std::unique_ptr<poly::AbstractRunner> runner;
+};
+
+void* ref_pbrt_load(const char* path) {
+    poly::pbrt_parser parser;
+    auto* r = new RefPbrt();
+    r->runner = parser.parse_file(path);
+    return r;
+}
+
+void ref_pbrt_free(void* h) { delete static_cast<RefPbrt*>(h); }
+
+// u[0..5] = width, height, spp, max_depth, number of shapes, has_env; f[0..2] = env;
+// f[3..12] = eye, look-at, up, fov; f[13..28] = camera-to-world matrix (row-major)
+void ref_pbrt_info(void* h, uint32_t* u, float* f) {
+    const poly::AbstractRunner& run = *static_cast<RefPbrt*>(h)->runner;
+    const poly::Scene& sc = *run.Scene;
+    u[0] = run.Bounds.x;
+    u[1] = run.Bounds.y;
+    u[2] = run.NumSamples;
+    u[3] = (uint32_t)run.Integrator->MaxDepth;
+    u[4] = (uint32_t)sc.Shapes.size();
+    const auto* sky = dynamic_cast<const poly::ColorSkybox*>(sc.Skybox.get());
+    u[5] = sky ? 1 : 0;
+    const poly::SpectralPowerDistribution env = sky ? sky->GetSpd(poly::Vector(0, 0, 1)) : poly::SpectralPowerDistribution();
+    f[0] = sky ? env.r : 0.f;
+    f[1] = sky ? env.g : 0.f;
+    f[2] = sky ? env.b : 0.f;
+    const poly::AbstractCamera& cam = *sc.Camera;
+    const float v[10] = {cam.eye.x, cam.eye.y, cam.eye.z, cam.lookAt.x, cam.lookAt.y, cam.lookAt.z,
+                         cam.up.x, cam.up.y, cam.up.z, cam.Settings.FieldOfView};
+    std::memcpy(f + 3, v, sizeof(v));
+    for (int k = 0; k < 16; ++k) f[13 + k] = cam.CameraToWorld.Matrix.Matrix[k / 4][k % 4];
+}
+
+// u[0..4] = vertices, faces, has normals, material type (0 = none), is light;
+// f[0..15] object-to-world, f[16..31] world-to-object, f[32..34] reflectance, f[35..37] radiance.
+// Arrays are copied when x is non-null.
+void ref_pbrt_mesh(void* h, uint32_t i, uint32_t* u, float* f, float* x, float* y, float* z, float* nx, float* ny,
+                   float* nz, uint32_t* fv0, uint32_t* fv1, uint32_t* fv2) {
+    const poly::Mesh& m = *static_cast<RefPbrt*>(h)->runner->Scene->Shapes[i];
+    const poly::mesh_geometry& g = *m.mesh_geometry;
+    u[0] = (uint32_t)g.x_packed.size();
+    u[1] = (uint32_t)g.fv0.size();
+    u[2] = g.has_vertex_normals ? 1 : 0;
+    u[3] = 0;
+    u[4] = m.is_light() ? 1 : 0;
+    for (int k = 0; k < 16; ++k) {
+        f[k] = m.object_to_world->Matrix.Matrix[k / 4][k % 4];
+        f[16 + k] = m.world_to_object->Matrix.Matrix[k / 4][k % 4];
+    }
+    f[32] = f[33] = f[34] = 0.f;
+    if (m.material && m.material->BRDF) {
+        u[3] = (uint32_t)m.material->BRDF->brdf_type;
+        if (const auto* l = dynamic_cast<const poly::LambertBRDF*>(m.material->BRDF.get())) {
+            f[32] = l->refl.r; f[33] = l->refl.g; f[34] = l->refl.b;
+        } else if (const auto* r = dynamic_cast<const poly::MirrorBRDF*>(m.material->BRDF.get())) {
+            f[32] = r->refl.r; f[33] = r->refl.g; f[34] = r->refl.b;
+        }
+    }
+    f[35] = m.spd ? m.spd->r : 0.f;
+    f[36] = m.spd ? m.spd->g : 0.f;
+    f[37] = m.spd ? m.spd->b : 0.f;
+    if (!x) return;
+    std::memcpy(x, g.x_packed.data(), 4 * g.x_packed.size());
+    std::memcpy(y, g.y_packed.data(), 4 * g.y_packed.size());
+    std::memcpy(z, g.z_packed.data(), 4 * g.z_packed.size());
+    std::memcpy(fv0, g.fv0.data(), 4 * g.fv0.size());
+    std::memcpy(fv1, g.fv1.data(), 4 * g.fv1.size());
+    std::memcpy(fv2, g.fv2.data(), 4 * g.fv2.size());
+    if (g.has_vertex_normals && nx) {
+        std::memcpy(nx, g.nx_packed.data(), 4 * g.nx_packed.size());
+        std::memcpy(ny, g.ny_packed.data(), 4 * g.ny_packed.size());
+        std::memcpy(nz, g.nz_packed.data(), 4 * g.nz_packed.size());
+    }
 }
 
 }  // extern "C"

@@ -119,6 +119,12 @@ class MeshData(C.Structure):
                 ("nx", _fp), ("ny", _fp), ("nz", _fp), ("u", _fp), ("v", _fp)]
 
 
+class PbrtInfo(C.Structure):
+    _fields_ = [("num_meshes", C.c_uint32), ("has_env", C.c_int32), ("env", C.c_float * 3),
+                ("width", C.c_uint32), ("height", C.c_uint32), ("spp", C.c_uint32), ("max_depth", C.c_uint32),
+                ("camera", Camera)]
+
+
 class RequestTiming(C.Structure):
     _fields_ = [("admitted_ms", C.c_double), ("first_wave_ms", C.c_double), ("last_wave_ms", C.c_double),
                 ("done_ms", C.c_double)]
@@ -155,6 +161,10 @@ def _load() -> C.CDLL:
         "pt_load_ply": (i, [C.c_char_p, C.POINTER(MeshData)]),
         "pt_mesh_data_free": (None, [C.POINTER(MeshData)]),
         "pt_write_png": (i, [C.c_char_p, _vp, u32, u32]),
+        "pt_load_pbrt": (i, [C.c_char_p, C.POINTER(_vp)]),
+        "pt_pbrt_get_info": (i, [_vp, C.POINTER(PbrtInfo)]),
+        "pt_pbrt_get_meshes": (i, [_vp, C.POINTER(C.POINTER(MeshDesc))]),
+        "pt_pbrt_free": (None, [_vp]),
         "pt_batch_default_tuning": (i, [C.POINTER(BatchTuning)]),
         "pt_batch_create": (i, [C.POINTER(BatchItem), u32, C.POINTER(BatchTuning), C.POINTER(_vp)]),
         "pt_batch_run": (i, [_vp, _vp]),
@@ -402,6 +412,53 @@ def load_ply(path: str, **mesh_kwargs) -> Mesh:
     m = Mesh(x, y, z, faces, normals=normals, **mesh_kwargs)
     m.uv = uv
     return m
+
+
+@dataclass
+class PbrtScene:
+    """A PBRT scene file as read by pt_load_pbrt: meshes (Scene::Shapes order), the environment
+    (None without LightSource "infinite") and the render settings of its scene block."""
+    meshes: list
+    env: Optional[tuple]
+    width: int
+    height: int
+    spp: int
+    max_depth: int
+    camera: dict
+
+    def render_args(self) -> dict:
+        return dict(width=self.width, height=self.height, spp=self.spp, max_depth=self.max_depth, camera=self.camera)
+
+
+def load_pbrt(path: str) -> PbrtScene:
+    """A PBRT scene file (pt_load_pbrt), copied into Mesh objects (instances share nothing here)."""
+    h = C.c_void_p()
+    check(lib.pt_load_pbrt(str(path).encode(), C.byref(h)))
+    try:
+        info = PbrtInfo()
+        check(lib.pt_pbrt_get_info(h, C.byref(info)))
+        descs = C.POINTER(MeshDesc)()
+        check(lib.pt_pbrt_get_meshes(h, C.byref(descs)))
+        meshes = []
+        for k in range(info.num_meshes):
+            d = descs[k]
+            nv, nf = d.num_vertices, d.num_faces
+            arr = lambda ptr, n, dt: np.ctypeslib.as_array(ptr, (n,)).astype(dt, copy=True) if n else np.zeros(0, dt)
+            x, y, z = (arr(getattr(d, c), nv, np.float32) for c in ("x", "y", "z"))
+            faces = np.stack([arr(getattr(d, c), nf, np.uint32) for c in ("fv0", "fv1", "fv2")], 1) if nf \
+                else np.zeros((0, 3), np.uint32)
+            normals = np.stack([arr(getattr(d, c), nv, np.float32) for c in ("nx", "ny", "nz")], 1) if bool(d.nx) else None
+            meshes.append(Mesh(x, y, z, faces,
+                               object_to_world=np.array(d.object_to_world[:], np.float32).reshape(4, 4),
+                               world_to_object=np.array(d.world_to_object[:], np.float32).reshape(4, 4),
+                               material=int(d.material), albedo=tuple(d.albedo[:]), is_light=bool(d.is_light),
+                               emission=tuple(d.emission[:]), normals=normals))
+        cam = dict(eye=tuple(info.camera.eye[:]), look_at=tuple(info.camera.look_at[:]), up=tuple(info.camera.up[:]),
+                   fov=float(info.camera.fov_deg))
+        env = tuple(info.env[:]) if info.has_env else None
+        return PbrtScene(meshes, env, info.width, info.height, info.spp, info.max_depth, cam)
+    finally:
+        lib.pt_pbrt_free(h)
 
 
 def film_to_rgba8(rgb_dev_ptr: int, width: int, height: int) -> np.ndarray:
