@@ -271,7 +271,8 @@ int prepare_scene_host(const pt_scene_desc* desc, HostScene& h) {
         h.meshes[m].is_light = d.is_light ? 1 : 0;
         std::memcpy(h.meshes[m].albedo, d.albedo, sizeof(d.albedo));
         std::memcpy(h.meshes[m].emission, d.emission, sizeof(d.emission));
-        if (d.nx && d.ny && d.nz) any_normals = true;
+        h.meshes[m].has_normals = (d.nx && d.ny && d.nz) ? 1 : 0;
+        if (h.meshes[m].has_normals) any_normals = true;
     }
     if (any_normals) {  // world vertex normals per prim (Transform::ApplyInPlace(Normal&), mesh.cpp:388-400)
         h.normals.assign(9 * (size_t)w.num_prims, 0.f);

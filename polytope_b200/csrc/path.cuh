@@ -50,7 +50,10 @@ PT_HD bool shade_hit(const RenderParams& p, PathState& s, uint32_t prim, uint32_
     }
     if (s.bounces >= p.max_depth) return false;
     const uint32_t bounce = s.bounces++;
-    const HitFrame fr = hit_frame(v0, v1, v2, u, v, w, s.d, p.prim_normals ? p.prim_normals + 9 * (size_t)prim : nullptr);
+    // interpolated vertex normals only for meshes that have them (Mesh::intersect, mesh.cpp:385-410:
+    // per mesh, so a scene can mix meshes with and without normals)
+    const HitFrame fr = hit_frame(v0, v1, v2, u, v, w, s.d,
+                                  (p.prim_normals && mr.has_normals) ? p.prim_normals + 9 * (size_t)prim : nullptr);
     uint32_t r[4] = {pixel, sample, bounce, 0u};
     philox4x32(r, p.seed_lo, p.seed_hi);
     const F3 d = s.d;

@@ -54,6 +54,7 @@ struct DeviceMesh {  // per-mesh shading record (device)
     int32_t is_light;
     float albedo[3];
     float emission[3];
+    int32_t has_normals;  // the mesh has vertex normals (mesh_geometry::has_vertex_normals)
 };
 
 struct HostScene {  // host copy of everything a scene handle uploads

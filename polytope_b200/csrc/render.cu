@@ -21,6 +21,9 @@
 #include "path.cuh"
 #include "wavefront.h"
 
+static_assert(sizeof(pt::MeshRec) == sizeof(pt::DeviceMesh) && alignof(pt::MeshRec) == alignof(pt::DeviceMesh),
+              "the kernels' mesh record must match the uploaded one");
+
 namespace pt {
 
 __global__ void __launch_bounds__(128) path_kernel(const RenderParams p, uint64_t first, uint32_t count,

@@ -113,11 +113,12 @@ PT_HD void load_face(const float4* __restrict__ tris, uint32_t leaf, F3& v0, F3&
     mesh = fbits(q2.z);
 }
 
-struct MeshRec {
+struct MeshRec {  // DeviceMesh, as the kernels read it
     uint32_t material;
     int32_t is_light;
     float albedo[3];
     float emission[3];
+    int32_t has_normals;
 };
 
 // Area-light sample for NEE at a Lambert vertex: returns true with the (unoccluded) contribution
