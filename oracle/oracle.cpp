@@ -515,11 +515,21 @@ public:
                     cn.offset = (uint32_t)leaf.size();
                     // bvh.cpp:666-671: the reference comparator (kept as is, including its
                     // lhs.first < lhs.second branch) decides the in-leaf order through std::sort.
-                    std::sort(tn.indices.begin(), tn.indices.end(),
-                              [](const std::pair<uint32_t, uint32_t>& l, const std::pair<uint32_t, uint32_t>& r) {
-                                  if (l.first == r.first) return l.second < r.second;
-                                  return l.first < l.second;
-                              });
+                    // It is not a strict weak order across meshes; std::sort stays in bounds with
+                    // it only on 16 elements or fewer (insertion sort), so a longer leaf mixing
+                    // meshes -- undefined in the reference -- is sorted by (mesh, face), the
+                    // library's defined choice.
+                    bool mixed = false;
+                    for (const auto& p : tn.indices) mixed = mixed || p.first != tn.indices[0].first;
+                    if (tn.indices.size() > 16 && mixed) {
+                        std::sort(tn.indices.begin(), tn.indices.end());
+                    } else {
+                        std::sort(tn.indices.begin(), tn.indices.end(),
+                                  [](const std::pair<uint32_t, uint32_t>& l, const std::pair<uint32_t, uint32_t>& r) {
+                                      if (l.first == r.first) return l.second < r.second;
+                                      return l.first < l.second;
+                                  });
+                    }
                     for (const auto& p : tn.indices) leaf.push_back(p);
                     cn.num_faces = (uint16_t)tn.indices.size();
                     last_ret = 0;

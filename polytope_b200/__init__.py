@@ -269,12 +269,13 @@ def mesh_descs(meshes: Sequence[Mesh]):
 def bvh_build(meshes: Sequence[Mesh], threads: int = 0):
     """The reference SAH BVH (node-for-node identical): returns (nodes, leaf_pairs)."""
     arr, keep = mesh_descs(meshes)
-    n = C.c_uint32(0)
-    check(lib.pt_bvh_build(arr, len(meshes), threads, None, C.byref(n), None))
+    faces = sum(len(m.faces) for m in meshes)
+    # one build: a tree over F faces has at most 2F - 1 nodes
+    n = C.c_uint32(max(1, 2 * faces - 1))
     nodes = np.zeros(n.value, NODE_DTYPE)
-    pairs = np.zeros((sum(len(m.faces) for m in meshes), 2), np.uint32)
+    pairs = np.zeros((faces, 2), np.uint32)
     check(lib.pt_bvh_build(arr, len(meshes), threads, nodes.ctypes.data, C.byref(n), _u(pairs)))
-    return nodes, pairs
+    return nodes[:n.value].copy(), pairs
 
 
 def _ptr(a) -> int:

@@ -16,6 +16,7 @@
 #include <cstring>
 #include <future>
 #include <limits>
+#include <memory>
 #include <thread>
 
 #include "pt_internal.h"
@@ -55,12 +56,20 @@ inline float box_area(const Box& b) {
     return (2 * x * y) + (2 * y * z) + (2 * z * x);
 }
 
-struct Node {
+struct Node {  // trivial, so the 2n-node pool is allocated without being initialised
     Box bb;
-    int32_t low = -1, high = -1;
-    uint16_t axis = 0;
-    uint32_t begin = 0, end = 0;  // element range (meaningful for leaves)
+    int32_t low, high;            // -1: leaf
+    uint16_t axis;
+    uint32_t begin, end;          // element range
 };
+
+inline void node_init(Node& n, const Box& bb, uint32_t begin, uint32_t end) {
+    n.bb = bb;
+    n.low = n.high = -1;
+    n.axis = 0;
+    n.begin = begin;
+    n.end = end;
+}
 
 struct Builder {
     const WorldMeshes& w;
@@ -69,7 +78,7 @@ struct Builder {
     std::vector<uint32_t> idx;    // element order (prim ids)
     std::vector<uint32_t> tmp;
     std::vector<uint8_t> bkt;
-    std::vector<Node> nodes;
+    std::unique_ptr<Node[]> nodes;
     std::atomic<uint32_t> next{0};
     int spawn_depth = 0;
 
@@ -111,7 +120,7 @@ struct Builder {
             const uint32_t p = idx[i];
             const float raw = (pcen[3 * (size_t)p + axis] - amin) / (float)width;
             unsigned bi = (unsigned)raw;
-            if (bi == 12) bi--;
+            if (bi >= 12) bi = 11;  // 12 at the top edge (the reference's bi--); NaN centroids stay in range
             bkt[i] = (uint8_t)bi;
             count[bi]++;
             box_union(bbox[bi], pbox[p]);
@@ -162,14 +171,8 @@ struct Builder {
         const uint32_t c = alloc2();
         high = c;
         low = c + 1;
-        Node& hn = nodes[high];
-        hn.bb = highbb[best + 1];
-        hn.begin = b + nlow;
-        hn.end = e;
-        Node& ln = nodes[low];
-        ln.bb = lowbb[best];
-        ln.begin = b;
-        ln.end = b + nlow;
+        node_init(nodes[high], highbb[best + 1], b + nlow, e);
+        node_init(nodes[low], lowbb[best], b, b + nlow);
         node.high = (int32_t)high;
         node.low = (int32_t)low;
         return true;
@@ -244,22 +247,37 @@ int bake_world(const pt_mesh_desc* meshes, uint32_t num_meshes, WorldMeshes& out
     out.num_prims = (uint32_t)total;
     out.tri.resize(9 * total);
     out.prim_mesh.resize(total);
-    for (uint32_t m = 0; m < num_meshes; ++m) {
-        const pt_mesh_desc& d = meshes[m];
-        for (uint32_t f = 0; f < d.num_faces; ++f) {
+    // every face independently, in parallel; the first bad face in prim order is the one reported
+    std::atomic<uint64_t> first_bad{~0ull};
+    parallel_ranges((size_t)total, 0, [&](size_t pb, size_t pe) {
+        uint32_t m = (uint32_t)(std::upper_bound(out.prim_base.begin(), out.prim_base.end(), (uint32_t)pb) -
+                                out.prim_base.begin()) - 1;
+        for (size_t p = pb; p < pe; ++p) {
+            while (m + 1 < num_meshes && p >= out.prim_base[m + 1]) ++m;
+            const pt_mesh_desc& d = meshes[m];
+            const uint32_t f = (uint32_t)(p - out.prim_base[m]);
             const uint32_t vi[3] = {d.fv0[f], d.fv1[f], d.fv2[f]};
-            float* t = &out.tri[9 * (size_t)(out.prim_base[m] + f)];
+            float* t = &out.tri[9 * p];
             for (int k = 0; k < 3; ++k) {
-                if (vi[k] >= d.num_vertices)
-                    return fail(PT_EINVAL, "mesh " + std::to_string(m) + " face " + std::to_string(f) +
-                                               ": vertex index out of range");
+                if (vi[k] >= d.num_vertices) {
+                    uint64_t cur = first_bad.load();
+                    while (p < cur && !first_bad.compare_exchange_weak(cur, p)) {}
+                    return;
+                }
                 t[3 * k + 0] = d.x[vi[k]];
                 t[3 * k + 1] = d.y[vi[k]];
                 t[3 * k + 2] = d.z[vi[k]];
                 apply_point(d.object_to_world, &t[3 * k]);
             }
-            out.prim_mesh[out.prim_base[m] + f] = m;
+            out.prim_mesh[p] = m;
         }
+    });
+    if (first_bad.load() != ~0ull) {
+        const uint64_t p = first_bad.load();
+        const uint32_t m = (uint32_t)(std::upper_bound(out.prim_base.begin(), out.prim_base.end(), (uint32_t)p) -
+                                      out.prim_base.begin()) - 1;
+        return fail(PT_EINVAL, "mesh " + std::to_string(m) + " face " + std::to_string(p - out.prim_base[m]) +
+                                   ": vertex index out of range");
     }
     return PT_OK;
 }
@@ -267,36 +285,44 @@ int bake_world(const pt_mesh_desc* meshes, uint32_t num_meshes, WorldMeshes& out
 int build_bvh(const pt_mesh_desc* meshes, uint32_t num_meshes, const WorldMeshes& w, int threads, BuiltTree& out) {
     const uint32_t n = w.num_prims;
     if (n == 0) return fail(PT_EINVAL, "scene has no faces (the reference's bvh::bound is undefined for it)");
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     Builder B(w);
     B.pbox.resize(n);
     B.pcen.resize(3 * (size_t)n);
-    Node root;
-    box_empty(root.bb);
-    for (uint32_t p = 0; p < n; ++p) {  // face boxes, centroids and the root box (bvh.cpp:53-121)
-        const float* t = &w.tri[9 * (size_t)p];
-        Box& b = B.pbox[p];
+    // face boxes and centroids (bvh.cpp:53-121), each face on its own, in parallel
+    parallel_ranges(n, threads, [&](size_t pb, size_t pe) {
+        for (size_t p = pb; p < pe; ++p) {
+            const float* t = &w.tri[9 * p];
+            Box& b = B.pbox[p];
+            for (int k = 0; k < 3; ++k) {
+                float mn = t[k] < t[3 + k] ? t[k] : t[3 + k];
+                mn = mn < t[6 + k] ? mn : t[6 + k];
+                float mx = t[k] > t[3 + k] ? t[k] : t[3 + k];
+                mx = mx > t[6 + k] ? mx : t[6 + k];
+                b.lo[k] = mn;
+                b.hi[k] = mx;
+                B.pcen[3 * p + k] = (mn + mx) * .5f;
+            }
+        }
+    });
+    // the root box folds the face boxes in element order, on one thread, so that ties (and signed
+    // zeros, and NaN) resolve exactly as in the reference's sequential loop
+    Box root_bb;
+    box_empty(root_bb);
+    for (uint32_t p = 0; p < n; ++p) {
+        const Box& b = B.pbox[p];
         for (int k = 0; k < 3; ++k) {
-            float mn = t[k] < t[3 + k] ? t[k] : t[3 + k];
-            mn = mn < t[6 + k] ? mn : t[6 + k];
-            float mx = t[k] > t[3 + k] ? t[k] : t[3 + k];
-            mx = mx > t[6 + k] ? mx : t[6 + k];
-            b.lo[k] = mn;
-            b.hi[k] = mx;
-            root.bb.lo[k] = root.bb.lo[k] < mn ? root.bb.lo[k] : mn;
-            root.bb.hi[k] = root.bb.hi[k] > mx ? root.bb.hi[k] : mx;
-            B.pcen[3 * (size_t)p + k] = (mn + mx) * .5f;
+            root_bb.lo[k] = root_bb.lo[k] < b.lo[k] ? root_bb.lo[k] : b.lo[k];
+            root_bb.hi[k] = root_bb.hi[k] > b.hi[k] ? root_bb.hi[k] : b.hi[k];
         }
     }
     B.idx.resize(n);
     for (uint32_t p = 0; p < n; ++p) B.idx[p] = p;  // master_indices order (mesh, then face)
     B.tmp.resize(n);
     B.bkt.resize(n);
-    B.nodes.resize(2 * (size_t)n);
-    root.begin = 0;
-    root.end = n;
-    B.nodes[0] = root;
+    B.nodes.reset(new Node[2 * (size_t)n]);
+    node_init(B.nodes[0], root_bb, 0, n);
     B.next.store(1);
-    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
     int sd = 0;
     while ((1 << sd) < threads) ++sd;
     B.spawn_depth = threads > 1 ? sd + 1 : 0;
@@ -304,13 +330,12 @@ int build_bvh(const pt_mesh_desc* meshes, uint32_t num_meshes, const WorldMeshes
 
     // compact_helper (bvh.cpp:652-693): pre-order DFS, low child at index + 1, high child at
     // index + high_child_offset; leaves append their (sorted) pairs to leaf_ordered_indices.
+    // Every node's output position is known up front -- its pre-order index follows from the
+    // subtree sizes, and a leaf's pairs start at its first element (the stable partition keeps the
+    // leaves' elements in pre-order), so subtrees are written in parallel with the same result.
     const uint32_t total_nodes = B.next.load();
     out.nodes.assign(total_nodes, pt_bvh_node{});
-    out.leaf_pairs.clear();
-    out.leaf_pairs.reserve(2 * (size_t)n);
-    struct Item { uint32_t tn, index, depth; };
-    std::vector<Item> st;
-    st.push_back({0, 0, 0});
+    out.leaf_pairs.assign(2 * (size_t)n, 0u);
     std::vector<uint32_t> sub(total_nodes, 0);
     // subtree sizes (descendant counts) by a reverse pass: children are always allocated after
     // their parent, so a descending sweep sees children first.
@@ -318,36 +343,94 @@ int build_bvh(const pt_mesh_desc* meshes, uint32_t num_meshes, const WorldMeshes
         const Node& nd = B.nodes[i];
         if (nd.low >= 0) sub[i] = 2 + sub[nd.low] + sub[nd.high];
     }
-    std::vector<std::pair<uint32_t, uint32_t>> leaf;
-    uint32_t max_depth = 0;
-    while (!st.empty()) {
-        const Item it = st.back();
-        st.pop_back();
+    struct Item { uint32_t tn, index, depth; };
+    std::atomic<bool> leaf_too_big{false};
+    // writes one node; returns true for an interior node, whose children the caller visits
+    auto emit = [&](const Item& it, std::vector<std::pair<uint32_t, uint32_t>>& leaf) {
         const Node& nd = B.nodes[it.tn];
         pt_bvh_node& cn = out.nodes[it.index];
         for (int k = 0; k < 3; ++k) { cn.bb_min[k] = nd.bb.lo[k]; cn.bb_max[k] = nd.bb.hi[k]; }
         cn.axis = nd.axis;
-        max_depth = std::max(max_depth, it.depth);
         if (nd.low < 0) {
-            cn.offset = (uint32_t)(out.leaf_pairs.size() / 2);
+            cn.offset = nd.begin;
             leaf.clear();
             for (uint32_t i = nd.begin; i < nd.end; ++i) {
                 const uint32_t p = B.idx[i];
                 const uint32_t m = w.prim_mesh[p];
                 leaf.emplace_back(m, p - w.prim_base[m]);
             }
-            std::sort(leaf.begin(), leaf.end(), LeafLess());
-            for (const auto& pr : leaf) { out.leaf_pairs.push_back(pr.first); out.leaf_pairs.push_back(pr.second); }
+            if (leaf.size() > 65535) {  // the 16-bit num_faces of the record cannot hold it
+                leaf_too_big.store(true);
+                return false;
+            }
+            // LeafLess is not a strict weak order when meshes differ.  libstdc++'s std::sort only
+            // runs its bounds-safe insertion sort on 16 elements or fewer; on a longer leaf that
+            // mixes meshes its unguarded partition can step past the leaf (undefined behaviour in
+            // the reference, which crashes on such scenes), so those leaves are sorted by (mesh,
+            // face) instead.
+            bool mixed = false;
+            for (const auto& pr : leaf) mixed = mixed || pr.first != leaf[0].first;
+            if (leaf.size() > 16 && mixed) std::sort(leaf.begin(), leaf.end());
+            else std::sort(leaf.begin(), leaf.end(), LeafLess());
+            uint32_t* dst = &out.leaf_pairs[2 * (size_t)nd.begin];
+            for (const auto& pr : leaf) { *dst++ = pr.first; *dst++ = pr.second; }
             cn.num_faces = (uint16_t)leaf.size();
-            continue;
+            return false;
         }
-        const uint32_t low_count = 1u + sub[nd.low];
-        cn.offset = low_count + 1;
+        cn.offset = 2 + sub[nd.low];
         cn.num_faces = 0;
-        // push high first so the low subtree is emitted first (pre-order, low then high)
-        st.push_back({(uint32_t)nd.high, it.index + 1 + low_count, it.depth + 1});
-        st.push_back({(uint32_t)nd.low, it.index + 1, it.depth + 1});
+        return true;
+    };
+    auto children = [&](const Item& it, Item& lo, Item& hi) {
+        const Node& nd = B.nodes[it.tn];
+        lo = {(uint32_t)nd.low, it.index + 1, it.depth + 1};
+        hi = {(uint32_t)nd.high, it.index + 2 + sub[nd.low], it.depth + 1};
+    };
+    // the top of the tree on this thread, down to subtrees of at most `grain` nodes
+    const uint32_t grain = std::max<uint32_t>(4096, total_nodes / (uint32_t)(8 * threads));
+    std::vector<Item> tasks, st{{0, 0, 0}};
+    std::vector<std::pair<uint32_t, uint32_t>> leaf;
+    uint32_t max_depth = 0;
+    while (!st.empty()) {
+        const Item it = st.back();
+        st.pop_back();
+        if (sub[it.tn] + 1 <= grain) { tasks.push_back(it); continue; }
+        max_depth = std::max(max_depth, it.depth);
+        if (!emit(it, leaf)) continue;
+        Item lo, hi;
+        children(it, lo, hi);
+        st.push_back(hi);
+        st.push_back(lo);
     }
+    std::atomic<size_t> next_task{0};
+    std::atomic<uint32_t> deepest{max_depth};
+    auto worker = [&]() {
+        std::vector<Item> stack;
+        std::vector<std::pair<uint32_t, uint32_t>> lp;
+        uint32_t dmax = 0;
+        for (size_t t; (t = next_task.fetch_add(1)) < tasks.size();) {
+            stack.assign(1, tasks[t]);
+            while (!stack.empty()) {
+                const Item it = stack.back();
+                stack.pop_back();
+                dmax = std::max(dmax, it.depth);
+                if (!emit(it, lp)) continue;
+                Item lo, hi;
+                children(it, lo, hi);
+                stack.push_back(hi);
+                stack.push_back(lo);
+            }
+        }
+        uint32_t cur = deepest.load();
+        while (dmax > cur && !deepest.compare_exchange_weak(cur, dmax)) {}
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
+    worker();
+    for (std::thread& th : pool) th.join();
+    max_depth = deepest.load();
+    if (leaf_too_big.load())
+        return fail(PT_EINVAL, "a leaf would hold more than 65535 faces (faces whose centroids coincide)");
     out.max_depth = max_depth;
     (void)meshes;
     (void)num_meshes;

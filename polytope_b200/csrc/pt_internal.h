@@ -3,9 +3,11 @@
 
 #include <cstdint>
 #include <cstddef>
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/polytope_b200.h"
@@ -20,6 +22,22 @@ void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);  // sets the message, returns code
 
 // ---- host BVH build (identical to the reference) ------------------------------------------------
+// Runs f(begin, end) over [0, n) split into contiguous ranges, one per thread (threads <= 0: one
+// per hardware thread), on the calling thread alone when the work is small.  Host-side helper for
+// per-element loops whose elements are independent.
+template <class F>
+void parallel_ranges(size_t n, int threads, F f) {
+    if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+    if (threads == 1 || n < 65536) {
+        f((size_t)0, n);
+        return;
+    }
+    const size_t chunk = (n + (size_t)threads - 1) / (size_t)threads;
+    std::vector<std::thread> pool;
+    for (size_t b = 0; b < n; b += chunk) pool.emplace_back(f, b, std::min(n, b + chunk));
+    for (std::thread& t : pool) t.join();
+}
+
 struct WorldMeshes {
     // world-space triangle of each global primitive id (9 floats), owning mesh and face
     std::vector<float> tri;        // 9 * num_prims

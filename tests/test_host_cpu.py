@@ -93,6 +93,43 @@ def test_bvh_build_identical_to_oracle(threads):
         assert (pairs == op).all()
 
 
+def coincident_soup(seed=0):
+    """Two meshes whose many degenerate faces share one centroid: leaves of more than 16 faces that
+    mix meshes, where the reference's std::sort with its leaf comparator is undefined."""
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(3000, 3)).astype(np.float32)
+    v[::7] = 0.0
+    v[1::11] *= -0.0
+    return [pb.Mesh(v[:, 0], v[:, 1], v[:, 2], rng.integers(0, 3000, (20000, 3))),
+            pb.Mesh(v[:, 0], v[:, 1], v[:, 2], rng.integers(0, 3000, (500, 3)),
+                    object_to_world=np.diag([1, -1, 1, 1]).astype(np.float32))]
+
+
+@pytest.mark.parametrize("threads", [1, 0])
+def test_long_mixed_leaves_build_safely_and_match_the_oracle(threads):
+    meshes = coincident_soup()
+    nodes, pairs = pb.bvh_build(meshes, threads=threads)
+    big = nodes[nodes["num_faces"] > 16]
+    assert len(big) > 0
+    mixed = 0
+    for nd in big:
+        leaf = pairs[nd["offset"]:nd["offset"] + nd["num_faces"]]
+        if len(set(leaf[:, 0])) > 1:  # the defined order: by (mesh, face)
+            mixed += 1
+            assert [tuple(p) for p in leaf] == sorted(tuple(p) for p in leaf)
+    assert mixed > 0
+    on, op = po.OracleScene(meshes).tree()
+    assert nodes.tobytes() == on.tobytes() and (pairs == op).all()
+
+
+def test_leaf_beyond_the_record_limit_is_refused():
+    z = np.zeros(3, np.float32)
+    m = pb.Mesh(z, z, z, np.zeros((70000, 3), np.uint32))  # 70,000 copies of one point-face
+    with pytest.raises(pb.PolytopeError) as e:
+        pb.bvh_build([m])
+    assert e.value.code == pb.PT_EINVAL and "65535" in str(e.value)
+
+
 def test_bvh_build_matches_reference_fixtures():
     g = load_golden("small_scene.npz")
     meshes, _ = W.small_scene()
