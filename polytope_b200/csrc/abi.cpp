@@ -79,6 +79,8 @@ bool is_pinned(const void* p) {
     return attr.type == cudaMemoryTypeHost;
 }
 
+// Rays per chunk of the host-pointer pipeline.  Measured on the 16.7 M-ray microbench end to end:
+// 1 M-ray chunks 1436 Mrays/s, 512 K 1413, 2 M 1339 (longer fill and drain), 256 K 1030.
 constexpr size_t kChunkRays = size_t(1) << 20;
 constexpr int kSlots = 4;  // chunks in flight: one being copied in, one or two in kernels, one copied out
 
