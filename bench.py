@@ -454,6 +454,9 @@ def main():
     ap.add_argument("--render-probe", action="store_true",
                     help="render the instanced scene at 480x270, 16 spp once with the plain launch and once with "
                          "the persistent path kernel, then exit (a small case for profilers)")
+    ap.add_argument("--batch-probe", action="store_true",
+                    help="run the first 32 scenes of the 256-scene batch once through the wavefront pipeline with "
+                         "the tuning the autotuner picks for the full batch, then exit (a small case for profilers)")
     ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
 
@@ -472,6 +475,21 @@ def main():
         for fl in (0, pb.RENDER_PERSISTENT):
             rgb, _ = pb.render(scene, 480, 270, 16, d["max_depth"], d["camera"], d["seed"], pb.RENDER_NEE | fl)
             print(json.dumps({"render_probe": "480x270x16", "flags": pb.RENDER_NEE | fl, "mean": float(rgb.mean())}))
+        return
+
+    if args.batch_probe:
+        import polytope_b200 as pb
+        from polytope_b200 import workloads as W
+        work = W.batched_workload(256)[:32]
+        scenes = build_scenes(pb, [(w[0], w[1]) for w in work])
+        jobs = [(sc, pb.render_desc(d["width"], d["height"], d["spp"], d["max_depth"], d["camera"], d["seed"], pb.RENDER_NEE))
+                for sc, (_, _, d) in zip(scenes, work)]
+        t = pb.default_tuning()
+        t.pipeline, t.wave_pixels, t.threads_per_block, t.stack_depth, t.queue_chunk = pb.PIPELINE_WAVEFRONT, 1 << 25, 256, 32, 32
+        b = pb.Batch(jobs, t)
+        b.run()
+        print(json.dumps({"batch_probe": "32 scenes, wavefront pipeline", "rays": int(b.rays_traced())}))
+        b.close()
         return
 
     import torch

@@ -12,8 +12,9 @@
 // and the wavefront extend/shadow kernel.  Measured on a B200 (each against the per-lane walk):
 // ray queries on the 1.3 M-face microbench 1722 -> 1985 Mrays/s at 16 (12: 1937, 24: slower);
 // whole paths on the 6.5 M-face frame 1595 -> 1678 Msamples/s at 12 (8 and 16 slower); the
-// wavefront kernel, held to 64 registers, lost 17 % to the vote's extra live state, so it walks
-// per lane.
+// wavefront kernel on the 256-scene batch 1806 -> 2024 Mrays/s at 12 with its first 16 stack
+// entries in shared memory (16: 1954, 20: 1801; with the stack in local memory the vote lost 17 %
+// at this kernel's 64 registers).
 #ifndef PT_LEAF_BATCH_TRACE
 #define PT_LEAF_BATCH_TRACE 16
 #endif
@@ -21,5 +22,5 @@
 #define PT_LEAF_BATCH_PATHS 12
 #endif
 #ifndef PT_LEAF_BATCH_WAVEFRONT
-#define PT_LEAF_BATCH_WAVEFRONT 0
+#define PT_LEAF_BATCH_WAVEFRONT 12
 #endif

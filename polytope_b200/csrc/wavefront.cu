@@ -69,8 +69,10 @@ __global__ void __launch_bounds__(128) wf_init_kernel(const WfItem* __restrict__
 // The first kWfTraceShared stack entries of a lane live in shared memory (blocks of up to 256
 // threads); kWfTraceMinBlocks is the resident-block floor given to the register allocator.
 // Measured on the 256-scene batch: 4 blocks of 256 (64 registers) beat the unconstrained 72
-// registers by 9 %; 5 or 6 blocks spill too much; a shared-memory stack changes little here.
-constexpr int kWfTraceShared = 0;
+// registers by 9 %, and 3 blocks or 5-6 blocks are slower; 16 shared entries together with the
+// warp-voted walk (PT_LEAF_BATCH_WAVEFRONT) gave 2024 Mrays/s against 1806 for neither (8 or 24
+// entries: 1918 / 1954 at batch 16; shared entries without the vote: no gain).
+constexpr int kWfTraceShared = 16;
 constexpr int kWfTraceMinBlocks = 4;
 
 template <int CAP, bool SHADOW>
