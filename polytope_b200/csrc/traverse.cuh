@@ -280,9 +280,11 @@ PT_HD bool walk_to_leaf(RayWalkT<CAP, SH>& k, const uint4* __restrict__ nodes, u
 // so that neither the node loop nor the face loop runs with a handful of lanes (stepping every
 // lane to its own next leaf left about 9 of 32 lanes busy on the 1.3 M-face microbench).
 // `walking` is this lane's eligibility at the start of the round; returns whether the lane walks
-// on, and sets at_leaf (faces to test in leaf_off / leaf_n) or ok = false (guard failure).
+// on, and sets at_leaf (faces to test in leaf_off / leaf_n) or ok = false (guard failure).  STEPS
+// node steps per ballot (a lane that reaches a leaf stops early): fewer votes, a little more
+// waiting; which is faster depends on the kernel.
 #ifdef __CUDACC__
-template <bool COUNT, int CAP, int SH>
+template <bool COUNT, int STEPS, int CAP, int SH>
 __device__ __forceinline__ void walk_round(RayWalkT<CAP, SH>& k, bool walking, int batch, const uint4* __restrict__ nodes,
                                            uint32_t num_nodes, bool& at_leaf, bool& ok, uint32_t& leaf_off,
                                            uint32_t& leaf_n) {
@@ -295,7 +297,10 @@ __device__ __forceinline__ void walk_round(RayWalkT<CAP, SH>& k, bool walking, i
         const uint32_t w = __ballot_sync(0xFFFFFFFFu, w_now);
         if (w == 0 || __popc(cand & ~w) >= want) break;
         if (w_now) {
-            const int r = walk_step<COUNT>(k, nodes, num_nodes, leaf_off, leaf_n);
+            int r = walk_step<COUNT>(k, nodes, num_nodes, leaf_off, leaf_n);
+#pragma unroll
+            for (int extra = 1; extra < STEPS; ++extra)
+                if (r == 0 && k.sp > 0) r = walk_step<COUNT>(k, nodes, num_nodes, leaf_off, leaf_n);
             at_leaf = r > 0;
             ok = r >= 0;
         }

@@ -143,8 +143,9 @@ __global__ void __launch_bounds__(256, kWfTraceMinBlocks) wf_trace_kernel(const 
         uint32_t leaf_off = 0, leaf_n = 0;
         bool ok, at_leaf;
         if constexpr (PT_LEAF_BATCH_WAVEFRONT > 0) {
-            walk_round<false>(k, active && k.sp > 0, PT_LEAF_BATCH_WAVEFRONT, nodes, num_nodes, at_leaf, ok, leaf_off,
-                              leaf_n);
+            // two node steps per ballot: 2152 vs 2028 Mrays/s on the 256-scene batch
+            walk_round<false, 2>(k, active && k.sp > 0, PT_LEAF_BATCH_WAVEFRONT, nodes, num_nodes, at_leaf, ok, leaf_off,
+                                 leaf_n);
         } else {
             ok = !active || walk_to_leaf<false, CAP>(k, nodes, num_nodes, leaf_off, leaf_n);
             at_leaf = active && ok && leaf_n > 0;
@@ -307,8 +308,9 @@ __global__ void __launch_bounds__(128, 8) wf_path_kernel(const WfItem* __restric
             uint32_t leaf_off = 0, leaf_n = 0;
             bool ok, at_leaf;
             if constexpr (PT_LEAF_BATCH_PATHS > 0) {
-                walk_round<false>(k, active && !finished && k.sp > 0, PT_LEAF_BATCH_PATHS, nodes, num_nodes, at_leaf, ok,
-                                  leaf_off, leaf_n);
+                // one node step per ballot: two measured 3 % slower here (1651 vs 1707 Msamples/s)
+                walk_round<false, 1>(k, active && !finished && k.sp > 0, PT_LEAF_BATCH_PATHS, nodes, num_nodes, at_leaf,
+                                     ok, leaf_off, leaf_n);
             } else {
                 const bool walking = active && !finished;
                 ok = !walking || walk_to_leaf<false>(k, nodes, num_nodes, leaf_off, leaf_n);
