@@ -251,6 +251,12 @@ typedef struct pt_mesh_data {
 /* ply_parser::parse_file (src/common/parsers/mesh_parsers.cpp:336-545): ascii and binary PLY.
  * Header errors and malformed data return PT_EINVAL with the reason. */
 int pt_load_ply(const char *path, pt_mesh_data *out);
+/* obj_parser::parse_file (src/common/parsers/mesh_parsers.cpp:547-598): Wavefront OBJ as the
+ * reference reads it -- every line whose first word starts with 'v' (vn and vt too) adds a vertex,
+ * every line starting with 'f' adds one triangle from its first three indices (the leading integer
+ * of each word, 1-based); other lines are ignored.  Unreadable numbers and indices outside the
+ * vertices return PT_EINVAL with the reason.  Release with pt_mesh_data_free. */
+int pt_load_obj(const char *path, pt_mesh_data *out);
 void pt_mesh_data_free(pt_mesh_data *mesh);
 
 /* poly::pbrt_parser::parse_file (src/common/parsers/pbrt_parser.cpp:284-1711): a PBRT scene file
@@ -263,9 +269,9 @@ void pt_mesh_data_free(pt_mesh_data *mesh);
  * most one LookAt (none: the identity camera, returned as LookAt (0,0,0) (0,0,1) (0,1,0), the same
  * matrix), Integrator "path", AttributeBegin/End, TransformBegin/End, Translate, Scale, Rotate,
  * Transform, Material "matte" / "mirror", MakeNamedMaterial / NamedMaterial, AreaLightSource
- * "diffuse", LightSource "infinite", Shape "plymesh" / "sphere", ObjectBegin / ObjectEnd /
- * ObjectInstance.  Textures, Material "plastic", Shape "objmesh" and other camera transforms are
- * rejected with PT_EINVAL and the reason; like the reference, other unknown directives are skipped.
+ * "diffuse", LightSource "infinite", Shape "plymesh" / "objmesh" / "sphere", ObjectBegin / ObjectEnd /
+ * ObjectInstance, Shape "objmesh" (pt_load_obj).  Textures, Material "plastic" and other camera
+ * transforms are rejected with PT_EINVAL and the reason; like the reference, other unknown directives are skipped.
  * A shape with neither a material nor an area light comes back with material 0, which
  * pt_scene_create rejects.  The mesh descriptions point into arrays owned by the handle
  * (instances share them) and stay valid until pt_pbrt_free. */

@@ -338,6 +338,19 @@ def ref_load_ply(path: str):
     return a[0], a[1], a[2], np.stack(fv, 1), normals
 
 
+def ref_load_obj(path: str):
+    """The reference's own obj_parser::parse_file (oracle/_ref): (x, y, z, faces)."""
+    lib = ref_lib()
+    f = lib.ref_load_obj
+    f.argtypes = [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)] + [C.c_void_p] * 6
+    nv, nf = C.c_uint32(0), C.c_uint32(0)
+    f(str(path).encode(), C.byref(nv), C.byref(nf), *([None] * 6))
+    a = [np.zeros(nv.value, np.float32) for _ in range(3)]
+    fv = [np.zeros(nf.value, np.uint32) for _ in range(3)]
+    f(str(path).encode(), C.byref(nv), C.byref(nf), *[v.ctypes.data for v in a + fv])
+    return a[0], a[1], a[2], np.stack(fv, 1) if nf.value else np.zeros((0, 3), np.uint32)
+
+
 def ref_load_pbrt(path: str) -> dict:
     """The reference's own pbrt_parser::parse_file (oracle/_ref) on a well-formed file: render
     settings, camera and, per shape, geometry, transforms, material and radiance."""

@@ -539,6 +539,24 @@ int ref_load_ply(const char* path, uint32_t* num_vertices, uint32_t* num_faces, 
     return 0;
 }
 
+int ref_load_obj(const char* path, uint32_t* num_vertices, uint32_t* num_faces, float* x, float* y, float* z,
+                 uint32_t* fv0, uint32_t* fv1, uint32_t* fv2) {
+    auto g = std::make_shared<poly::mesh_geometry>();
+    const poly::obj_parser parser;
+    parser.parse_file(g, path);
+    *num_vertices = (uint32_t)g->x_packed.size();
+    *num_faces = (uint32_t)g->fv0.size();
+    if (x) {
+        std::memcpy(x, g->x_packed.data(), 4 * g->x_packed.size());
+        std::memcpy(y, g->y_packed.data(), 4 * g->y_packed.size());
+        std::memcpy(z, g->z_packed.data(), 4 * g->z_packed.size());
+        std::memcpy(fv0, g->fv0.data(), 4 * g->fv0.size());
+        std::memcpy(fv1, g->fv1.data(), 4 * g->fv1.size());
+        std::memcpy(fv2, g->fv2.data(), 4 * g->fv2.size());
+    }
+    return 0;
+}
+
 // ---- the reference's PBRT scene parser (pbrt_parser.cpp), for the pt_load_pbrt parity tests ----
 // ref_pbrt_load parses a file with poly::pbrt_parser::parse_file and keeps the runner it returns;
 // the accessors copy out what the renderer would use.  A file the reference cannot parse ends the

@@ -159,6 +159,7 @@ def _load() -> C.CDLL:
         "pt_render_noalloc": (i, [_vp, C.POINTER(RenderDesc), _vp, _vp, _vp]),
         "pt_film_to_rgba8": (i, [_vp, u32, u32, _vp, u32, _vp]),
         "pt_load_ply": (i, [C.c_char_p, C.POINTER(MeshData)]),
+        "pt_load_obj": (i, [C.c_char_p, C.POINTER(MeshData)]),
         "pt_mesh_data_free": (None, [C.POINTER(MeshData)]),
         "pt_write_png": (i, [C.c_char_p, _vp, u32, u32]),
         "pt_load_pbrt": (i, [C.c_char_p, C.POINTER(_vp)]),
@@ -399,8 +400,17 @@ def render(scene: Scene, width: int, height: int, spp: int, max_depth: int, came
 def load_ply(path: str, **mesh_kwargs) -> Mesh:
     """A PLY file as a Mesh (pt_load_ply); keyword arguments go to Mesh (transform, material...).
     Vertex uv, when present, is in the returned mesh's `uv` attribute."""
+    return _load_mesh(lib.pt_load_ply, path, mesh_kwargs)
+
+
+def load_obj(path: str, **mesh_kwargs) -> Mesh:
+    """A Wavefront OBJ file as a Mesh (pt_load_obj, the reference's obj_parser rules)."""
+    return _load_mesh(lib.pt_load_obj, path, mesh_kwargs)
+
+
+def _load_mesh(loader, path, mesh_kwargs) -> Mesh:
     d = MeshData()
-    check(lib.pt_load_ply(str(path).encode(), C.byref(d)))
+    check(loader(str(path).encode(), C.byref(d)))
     try:
         nv, nf = d.num_vertices, d.num_faces
         arr = lambda p, n, dt: np.ctypeslib.as_array(p, (n,)).astype(dt, copy=True) if n else np.zeros(0, dt)

@@ -27,7 +27,7 @@
 //   * Shape "sphere" tessellates a UV sphere with max((int)radius, 20) meridians and parallels
 //     (the north pole is emitted twice, as the tessellator does) and ends with the active
 //     transform, not the radius-scaled one: the radius only sets the tessellation.
-//   * Inside ObjectBegin / ObjectEnd, plymesh shapes append to the object's geometry (face indices
+//   * Inside ObjectBegin / ObjectEnd, plymesh / objmesh shapes append to the object's geometry (face indices
 //     as written in each file) and a sphere replaces the block's current geometry without being
 //     recorded for the object; ObjectInstance makes one shape from the object's geometry with
 //     the active transform, material and light.
@@ -38,7 +38,7 @@
 // reference's lexer reads 15 and then fails), and a binary PLY without normals is read with one
 // vertex per file vertex (the PLY note in ply.cpp).  Not supported, with an error naming the
 // directive: textures (Texture, "texture Kd"), Material "plastic" (no glossy BRDF in the render
-// path), Shape "objmesh", and a camera whose scene block holds more than one LookAt or any other
+// path), and a camera whose scene block holds more than one LookAt or any other
 // transform (no LookAt is the identity camera, the same matrix as LookAt (0,0,0) (0,0,1) (0,1,0)).  Like the
 // reference, unknown directives, unknown shape types and lights other than "infinite" / area
 // "diffuse" are ignored.
@@ -472,11 +472,12 @@ struct pt_pbrt_scene {
 namespace pt {
 namespace {
 
-int read_ply_geometry(const std::string& path, Geometry& g, std::string& err) {
+// plymesh / objmesh geometry appended to g (mesh_geometry's add_vertex / add_packed_face).
+int read_mesh_geometry(const std::string& path, bool obj, Geometry& g, std::string& err) {
     pt_mesh_data md{};
-    const int rc = pt_load_ply(path.c_str(), &md);
+    const int rc = obj ? pt_load_obj(path.c_str(), &md) : pt_load_ply(path.c_str(), &md);
     if (rc) {
-        err = "plymesh [" + path + "]: " + pt_last_error();
+        err = std::string(obj ? "objmesh [" : "plymesh [") + path + "]: " + pt_last_error();
         return rc;
     }
     const bool normals = md.nx && md.ny && md.nz;
@@ -719,13 +720,13 @@ int load(const std::string& path, pt_pbrt_scene& out, std::string& err) {
             }
             make_shape(it->second);
         } else if (n == "Shape") {
-            if (d.type == "plymesh") {
+            if (d.type == "plymesh" || d.type == "objmesh") {
                 std::string file;
                 for (const Arg& a : d.args)
                     if (a.name == "filename" && !a.values.empty()) file = a.values[0];
                 if (file.empty()) continue;  // missing filename: the reference skips the shape
                 auto g = in_object ? current_geometry : std::make_shared<Geometry>();
-                if ((rc = read_ply_geometry(base + file, *g, err))) return rc;
+                if ((rc = read_mesh_geometry(base + file, d.type == "objmesh", *g, err))) return rc;
                 if (!in_object) make_shape(g);
             } else if (d.type == "sphere") {
                 for (const Arg& a : d.args) {
@@ -739,9 +740,6 @@ int load(const std::string& path, pt_pbrt_scene& out, std::string& err) {
                     if (in_object) current_geometry = g;
                     else make_shape(g);
                 }
-            } else if (d.type == "objmesh") {
-                err = "line " + std::to_string(d.line) + ": Shape \"objmesh\" is not supported";
-                return PT_EINVAL;
             }
         } else if (n == "Texture") {
             err = "line " + std::to_string(d.line) + ": Texture is not supported";

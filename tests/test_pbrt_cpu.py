@@ -213,7 +213,7 @@ def test_defaults_and_identity_camera(tmp_path):
     ('LookAt 0 0 5 0 0 0 0 1 0\nWorldBegin\nTexture "t" "color" "imagemap" "string filename" [ "a.png" ]\nWorldEnd\n',
      "Texture"),
     ('LookAt 0 0 5 0 0 0 0 1 0\nWorldBegin\nMaterial "plastic" "rgb Kd" [ .5 .5 .5 ]\nWorldEnd\n', "plastic"),
-    ('LookAt 0 0 5 0 0 0 0 1 0\nWorldBegin\nShape "objmesh" "string filename" [ "a.obj" ]\nWorldEnd\n', "objmesh"),
+    ('LookAt 0 0 5 0 0 0 0 1 0\nWorldBegin\nShape "objmesh" "string filename" [ "a.obj" ]\nWorldEnd\n', "a.obj"),
     ('Scale -1 1 1\nLookAt 0 0 5 0 0 0 0 1 0\nWorldBegin\nWorldEnd\n', "LookAt"),
     ('LookAt 0 0 5 0 0 0 0 1 0\nLookAt 0 0 5 0 0 0 0 1 0\nWorldBegin\nWorldEnd\n', "LookAt"),
     ('LookAt 0 0 5 0 0 0\nWorldBegin\nWorldEnd\n', "LookAt"),
