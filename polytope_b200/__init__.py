@@ -197,7 +197,8 @@ lib = _load()
 
 
 def last_error() -> str:
-    return lib.pt_last_error().decode()
+    # messages can quote bytes of a malformed input file, which need not be UTF-8
+    return lib.pt_last_error().decode("utf-8", errors="replace")
 
 
 def check(rc: int) -> None:

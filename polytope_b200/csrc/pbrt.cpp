@@ -734,6 +734,13 @@ int load(const std::string& path, pt_pbrt_scene& out, std::string& err) {
                     std::vector<float> v;
                     if ((rc = arg_floats(d, a, v, err))) return rc;
                     if (v.empty()) continue;
+                    // (int)radius steps per axis: a large radius would ask for an unbounded mesh (the
+                    // reference tries to build it); refuse beyond 2048 (8.4 M faces)
+                    if (!(v[0] < 2049.f)) {
+                        err = "line " + std::to_string(d.line) + ": sphere radius " + std::to_string(v[0]) +
+                              " would tessellate into more than 2048 x 2048 steps";
+                        return PT_EINVAL;
+                    }
                     auto g = std::make_shared<Geometry>();
                     const int sub = std::max((int)v[0], 20);
                     tessellate_sphere((unsigned)sub, (unsigned)sub, *g);

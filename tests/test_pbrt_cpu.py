@@ -227,3 +227,48 @@ def test_unsupported_or_malformed_files_are_rejected(tmp_path, text, why):
     with pytest.raises(pb.PolytopeError) as e:
         pb.load_pbrt(tmp_path / "bad.pbrt")
     assert e.value.code == pb.PT_EINVAL and why in str(e.value)
+
+
+def test_huge_sphere_radius_is_refused(tmp_path):
+    (tmp_path / "s.pbrt").write_text('LookAt 0 0 5 0 0 0 0 1 0\nWorldBegin\nMaterial "matte" "rgb Kd" [ .5 .5 .5 ]\n'
+                                     'Shape "sphere" "float radius" [ 1e9 ]\nWorldEnd\n')
+    with pytest.raises(pb.PolytopeError) as e:
+        pb.load_pbrt(tmp_path / "s.pbrt")
+    assert e.value.code == pb.PT_EINVAL and "sphere radius" in str(e.value)
+
+
+def test_mutated_files_fail_cleanly(tmp_path):
+    """Random byte mutations of valid scene, OBJ and PLY files: every load either succeeds or
+    raises PolytopeError (PT_EINVAL / PT_ENOMEM) -- never a crash or another exception."""
+    import random
+    from test_obj_cpu import write_obj
+    from test_ply_cpu import CASES, mesh_arrays
+    write_scene(tmp_path)
+    write_obj(tmp_path / "t.obj", 0)
+    fmt, props, ff = CASES[3]
+    v, faces = mesh_arrays(3)
+    write_ply(tmp_path / "t.ply", fmt, v, faces, props, ff)
+    seeds = {"pbrt": (tmp_path / "scene.pbrt").read_bytes(), "obj": (tmp_path / "t.obj").read_bytes(),
+             "ply": (tmp_path / "t.ply").read_bytes()}
+    rng = random.Random(7)
+    loaders = {"pbrt": pb.load_pbrt, "obj": pb.load_obj, "ply": pb.load_ply}
+    for it in range(150):
+        kind = ("pbrt", "obj", "ply")[it % 3]
+        b = bytearray(seeds[kind])
+        for _ in range(rng.randint(1, 6)):
+            i = rng.randrange(len(b))
+            r = rng.random()
+            if r < 0.4:
+                b[i] = rng.randrange(256)
+            elif r < 0.6:
+                del b[i:i + rng.randint(1, 40)]
+            else:
+                b[i:i] = rng.choice([b" [ ", b" ] ", b'"', b"\n", b" 1e38 ", b" -1 ", b" 4294967295 ", b" nan ",
+                                     b"AttributeEnd\n", b'ObjectInstance "x"\n'])
+        path = tmp_path / ("scene.pbrt" if kind == "pbrt" else f"fz.{kind}")
+        path.write_bytes(bytes(b))
+        try:
+            loaders[kind](path)
+        except pb.PolytopeError as e:
+            assert e.code in (pb.PT_EINVAL, pb.PT_ENOMEM)
+    (tmp_path / "scene.pbrt").write_bytes(seeds["pbrt"])
