@@ -44,6 +44,7 @@
 // "diffuse" are ignored.
 
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
