@@ -379,7 +379,7 @@ def ref_load_pbrt(path: str) -> dict:
             out["meshes"].append(dict(x=a[0], y=a[1], z=a[2], faces=np.stack(fv, 1) if nf else np.zeros((0, 3), np.uint32),
                                       normals=np.stack(a[3:], 1) if mu[2] else None, material=int(mu[3]),
                                       is_light=bool(mu[4]), object_to_world=mf[0:16].reshape(4, 4).copy(),
-                                      world_to_object=mf[16:32].reshape(4, 4).copy(), albedo=mf[32:35].copy(),
+                                      normal_inverse=mf[16:32].reshape(4, 4).copy(), albedo=mf[32:35].copy(),
                                       emission=mf[35:38].copy()))
         return out
     finally:

@@ -599,7 +599,8 @@ void ref_pbrt_info(void* h, uint32_t* u, float* f) {
 }
 
 // u[0..4] = vertices, faces, has normals, material type (0 = none), is light;
-// f[0..15] object-to-world, f[16..31] world-to-object, f[32..34] reflectance, f[35..37] radiance.
+// f[0..15] object-to-world, f[16..31] the inverse stored in the object-to-world transform (what
+// Mesh::intersect transforms vertex normals with), f[32..34] reflectance, f[35..37] radiance.
 // Arrays are copied when x is non-null.
 void ref_pbrt_mesh(void* h, uint32_t i, uint32_t* u, float* f, float* x, float* y, float* z, float* nx, float* ny,
                    float* nz, uint32_t* fv0, uint32_t* fv1, uint32_t* fv2) {
@@ -612,7 +613,7 @@ void ref_pbrt_mesh(void* h, uint32_t i, uint32_t* u, float* f, float* x, float* 
     u[4] = m.is_light() ? 1 : 0;
     for (int k = 0; k < 16; ++k) {
         f[k] = m.object_to_world->Matrix.Matrix[k / 4][k % 4];
-        f[16 + k] = m.world_to_object->Matrix.Matrix[k / 4][k % 4];
+        f[16 + k] = m.object_to_world->Inverse.Matrix[k / 4][k % 4];
     }
     f[32] = f[33] = f[34] = 0.f;
     if (m.material && m.material->BRDF) {

@@ -15,8 +15,10 @@
 //   * A shape keeps a pointer to the *active transform object*, and Translate / Rotate / Scale
 //     in the same attribute scope multiply into that object in place, so a transform that follows
 //     a shape also moves the shapes before it in that scope (AttributeBegin / TransformBegin start
-//     a new object, a copy of the current one).  The shape's world-to-object transform (used only
-//     for vertex normals) is the inverse taken when the shape is created.
+//     a new object, a copy of the current one).  Vertex normals go through the inverse stored in
+//     that same object, in its final state (Mesh::intersect, mesh.cpp:397-399, calls
+//     object_to_world->ApplyInPlace(Normal&), which reads the transform's Inverse matrix; the
+//     mesh's own world_to_object is never used), so pt_mesh_desc::world_to_object carries it.
 //   * Transform *= multiplies both the matrix and the stored inverse on the right (so the stored
 //     "inverse" of a composed transform is the product of the inverses in the same order), and
 //     Matrix4x4::Inverse picks pivots by integer-truncated magnitude (pivot_magnitude below).
@@ -456,7 +458,6 @@ struct Spd {
 struct Shape {
     std::shared_ptr<Geometry> geometry;
     std::shared_ptr<Xf> to_world;  // the shared, possibly later-mutated transform object
-    M4 to_object;                  // inverse taken when the shape was made
     std::shared_ptr<Material> material;
     std::shared_ptr<Spd> light;
 };
@@ -607,7 +608,6 @@ int load(const std::string& path, pt_pbrt_scene& out, std::string& err) {
         Shape s;
         s.geometry = g;
         s.to_world = active_xf;
-        s.to_object = active_xf->inv;  // Invert(): Transform(Inverse, Matrix)
         s.material = active_mat;
         s.light = active_light;
         shapes.push_back(s);
@@ -767,7 +767,7 @@ int load(const std::string& path, pt_pbrt_scene& out, std::string& err) {
         if (!g.nx.empty()) { m.nx = g.nx.data(); m.ny = g.ny.data(); m.nz = g.nz.data(); }
         for (int k = 0; k < 16; ++k) {
             m.object_to_world[k] = s.to_world->mat.m[k / 4][k % 4];
-            m.world_to_object[k] = s.to_object.m[k / 4][k % 4];
+            m.world_to_object[k] = s.to_world->inv.m[k / 4][k % 4];  // the normals' matrix
         }
         if (s.material) {
             m.material = s.material->type;

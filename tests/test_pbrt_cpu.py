@@ -103,7 +103,9 @@ def assert_same_as_reference(s, r):
             assert np.array_equal(getattr(a, k), b[k]), (i, k)
         assert np.array_equal(a.faces, b["faces"]), i
         assert np.array_equal(a.object_to_world, b["object_to_world"]), i
-        assert np.array_equal(a.world_to_object, b["world_to_object"]), i
+        # the matrix vertex normals are transformed with: the stored inverse of the (final)
+        # object-to-world transform, as Transform::ApplyInPlace(Normal&) reads it
+        assert np.array_equal(a.world_to_object, b["normal_inverse"]), i
         assert a.is_light == b["is_light"], i
         assert np.array_equal(np.float32(a.emission), b["emission"]), i
         if not a.is_light:
@@ -124,7 +126,7 @@ def test_generated_scene_reads_as_expected(tmp_path):
     # both lights share the scope's radiance and transform, updated after the first shape
     assert lights[0].emission == lights[1].emission == (5 * 255.0,) * 3
     assert np.array_equal(lights[0].object_to_world, lights[1].object_to_world)
-    assert not np.array_equal(lights[0].world_to_object, lights[1].world_to_object)
+    assert np.array_equal(lights[0].world_to_object, lights[1].world_to_object)
     # UV spheres: radius only sets the tessellation (max(int(r), 20) meridians and parallels)
     spheres = [m for m in s.meshes if m.material == pb.MAT_MIRROR]
     assert [len(m.faces) for m in spheres] == [2 * 20 * 20, 2 * 24 * 24]
