@@ -416,7 +416,7 @@ int pt_server_fetch(pt_server *server, uint64_t ticket, float *rgb_out, uint32_t
 int pt_server_get_stats(pt_server *server, pt_server_stats *stats);
 int pt_server_destroy(pt_server *server);
 
-/* ---- synthetic workload generators (deterministic, shared by the checker and the bench) --- */
+/* ---- synthetic workload generators (deterministic, shared by the oracle and the bench) --- */
 
 /* Icosphere: icosahedron subdivided `level` times (20 * 4^level faces, 10 * 4^level + 2
  * vertices) of the given radius, each vertex displaced radially by `noise_amp` times 3-octave

@@ -1,6 +1,6 @@
 // oracle.cpp -- CPU restatement of Polytope's ray/path-tracing hot path.
 //
-// TEST INFRASTRUCTURE ONLY.  This file is the checker the CUDA path is compared against; nothing in
+// TEST INFRASTRUCTURE ONLY.  This file is the oracle the CUDA path is compared against; nothing in
 // the product (polytope_b200/) links, loads or calls it.  It restates, function by function, the
 // reference algorithm (paths relative to the Polytope source tree):
 //

@@ -1,4 +1,4 @@
-"""ctypes bindings for the checker libraries.
+"""ctypes bindings for the oracle libraries.
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and bench.py's CPU
 baseline leg.  Two libraries are wrapped:

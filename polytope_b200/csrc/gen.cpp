@@ -1,6 +1,6 @@
 // gen.cpp -- deterministic synthetic workloads (the reference ships only a UV-sphere tessellator,
 // src/cpu/shapes/tesselators.cpp:10-84; the workloads here need an icosphere, value noise and
-// seeded ray sets, defined once in this file and fed identically to the checker and the GPU).
+// seeded ray sets, defined once in this file and fed identically to the oracle and the GPU).
 //
 // All arithmetic is double precision with correctly rounded operations (+ - * / sqrt), rounded to
 // float at the end, so the outputs are the same on every IEEE-754 host.

@@ -11,7 +11,7 @@
 // with the render-loop definitions the CPU checker shares: Philox4x32-10 keyed (pixel, sample,
 // bounce, block) for every random number, sin/cos(2 pi u) from exact_math.h, the frame computed
 // once from the mesh owning the hit face, and optional area-light NEE.  Every float operation is
-// the checker's, in its order, so images agree bit for bit.
+// the oracle's, in its order, so images agree bit for bit.
 #pragma once
 
 #include "render.h"
