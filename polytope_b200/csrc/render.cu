@@ -7,7 +7,7 @@
 //                compaction and one atomic per warp, and a shadow kernel (any hit).
 // Either way a resolve kernel then adds each pixel's samples to the film in sample order (the
 // order of BoxFilter::Output's sum, BoxFilter.cpp:54-71), so the film is deterministic and equal
-// to the CPU checker's bit for bit.
+// to the CPU oracle's bit for bit.
 
 #include <algorithm>
 #include <cstring>

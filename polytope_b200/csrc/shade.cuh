@@ -8,7 +8,7 @@
 //   LambertBRDF / CosineSampleHemisphere      src/cpu/shading/brdf/lambert_brdf.h:48-57, constants.h:106-115
 //   MirrorBRDF::sample                        src/cpu/shading/brdf/mirror_brdf.h:23-35
 //   PathTraceIntegrator::GetSample            src/cpu/integrators/PathTraceIntegrator.cpp:10-135
-// with the render-loop definitions the CPU checker shares: Philox4x32-10 keyed (pixel, sample,
+// with the render-loop definitions the CPU oracle shares: Philox4x32-10 keyed (pixel, sample,
 // bounce, block) for every random number, sin/cos(2 pi u) from exact_math.h, the frame computed
 // once from the mesh owning the hit face, and optional area-light NEE.  Every float operation is
 // the oracle's, in its order, so images agree bit for bit.

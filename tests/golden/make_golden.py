@@ -15,7 +15,7 @@ Two kinds of fixture:
 
 2. ``*.npz`` -- outputs of the reference itself (oracle/_ref/libpolyref.so: the unmodified
    bvh::bound / compact / intersect_compact / Mesh::intersect, and the patched render loop) on
-   the seeded synthetic workloads, at sizes the CPU checker finishes in seconds.
+   the seeded synthetic workloads, at sizes the CPU oracle finishes in seconds.
 
 Usage:  make -C oracle && python tests/golden/make_golden.py
 """
