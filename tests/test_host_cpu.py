@@ -83,7 +83,7 @@ def soup(seed, meshes=3, faces=2000):
     return out
 
 
-@pytest.mark.parametrize("threads", [1, 0])
+@pytest.mark.parametrize("threads", [1, 0, 3, 32])
 def test_bvh_build_identical_to_oracle(threads):
     for meshes in (W.small_scene()[0], soup(1), soup(2, meshes=1, faces=1)):
         nodes, pairs = pb.bvh_build(meshes, threads=threads)
@@ -120,6 +120,16 @@ def test_long_mixed_leaves_build_safely_and_match_the_oracle(threads):
     assert mixed > 0
     on, op = po.OracleScene(meshes).tree()
     assert nodes.tobytes() == on.tobytes() and (pairs == op).all()
+
+
+def test_parallel_build_is_deterministic():
+    """The parallel phases (baking, face boxes, subtree tasks, compaction) give the same bytes on
+    every run and for every thread count."""
+    meshes = W.instanced_scene(level=5)[0]
+    ref_nodes, ref_pairs = pb.bvh_build(meshes, threads=1)
+    for threads in (0, 2, 5, 16, 0, 16):
+        nodes, pairs = pb.bvh_build(meshes, threads=threads)
+        assert nodes.tobytes() == ref_nodes.tobytes() and pairs.tobytes() == ref_pairs.tobytes()
 
 
 def test_leaf_beyond_the_record_limit_is_refused():
