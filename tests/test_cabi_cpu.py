@@ -78,3 +78,20 @@ def test_c_and_cpp_callers(tmp_path, compiler, std):
     m = pb.load_ply(tmp_path / "blob.ply")
     assert lines[1].split() == [str(len(m.x)), str(len(m.faces)), "1"]
     assert lines[2] == pb.version()
+
+
+def test_render_example_builds_and_fails_cleanly_without_a_device(tmp_path):
+    """polytope_b200/examples/render_pbrt.cpp compiles against the header; here, without a CUDA
+    device, it stops at pt_scene_create with the library's PT_ECUDA message."""
+    import torch
+    if not shutil.which("g++"):
+        pytest.skip("g++ not available")
+    exe = tmp_path / "render_pbrt"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "polytope_b200", "examples", "render_pbrt.cpp"), "-o", str(exe),
+                    "-L", LIBDIR, "-lpolytope_b200", f"-Wl,-rpath,{LIBDIR}"], check=True, capture_output=True)
+    if torch.cuda.is_available():
+        pytest.skip("this checks the no-device path")
+    scene = write_scene(tmp_path)
+    p = subprocess.run([str(exe), str(scene), str(tmp_path / "out.png")], capture_output=True, text=True)
+    assert p.returncode == 1 and "pt_scene_create" in p.stderr and "no CUDA device" in p.stderr
