@@ -362,6 +362,40 @@ int pt_batch_destroy(pt_batch *batch);
 int pt_batch_autotune(const pt_batch_item *items, uint32_t n, pt_batch_tuning *best, double *best_ms,
                       pt_batch_tune_result *results, uint32_t *num_results);
 
+/* ---- autotuner cache (no counterpart in the reference) ------------------------------------ */
+
+/* The class of a batch that a cached tuning is reused for: the device and the workload's scale.
+ * Two batches of one class share a tuning; the sizes are bucketed by powers of two. */
+typedef struct pt_tuning_class {
+    char     device[64];          /* cudaDeviceProp::name, NUL-terminated                       */
+    uint32_t sm_count;
+    uint32_t compute_capability;  /* major * 10 + minor                                          */
+    uint32_t items_log2;          /* floor(log2(number of renders))                              */
+    uint32_t pixels_log2;         /* floor(log2(sum of width * height))                          */
+    uint32_t samples_log2;        /* floor(log2(sum of width * height * spp))                    */
+    uint32_t faces_log2;          /* floor(log2(faces of the distinct scenes))                   */
+    uint32_t tree_depth;          /* deepest tree level of the scenes (decides the stacks that fit) */
+    uint32_t max_depth;           /* largest path depth                                          */
+    uint32_t flags;               /* OR of the renders' PT_RENDER_* flags                        */
+} pt_tuning_class;
+
+/* The class of a batch (the scenes' device must be present: PT_ECUDA otherwise). */
+int pt_tuning_class_of(const pt_batch_item *items, uint32_t n, pt_tuning_class *cls);
+/* Looks a class up in the JSON cache file at `path`: *found = 1 and the stored tuning and time,
+ * or *found = 0 (also when the file does not exist).  A file that is not a tuning cache, or holds
+ * an entry whose values pt_batch_create would refuse, returns PT_EINVAL with the reason. */
+int pt_tuning_cache_get(const char *path, const pt_tuning_class *cls, pt_batch_tuning *tuning, double *ms,
+                        int *found);
+/* Stores (or replaces) the class's entry.  Safe against concurrent writers in other threads and
+ * processes (an exclusive flock on "<path>.lock", then a temporary file renamed over the old one);
+ * a file that is not a tuning cache is left untouched and reported with PT_EINVAL. */
+int pt_tuning_cache_put(const char *path, const pt_tuning_class *cls, const pt_batch_tuning *tuning, double ms);
+/* pt_batch_autotune through the cache: the stored tuning of the batch's class when there is one
+ * (*from_cache = 1, no timing runs), otherwise the search, whose result is stored before return.
+ * If storing fails, *best is still set and the call returns the file's error. */
+int pt_batch_autotune_cached(const pt_batch_item *items, uint32_t n, const char *path, pt_batch_tuning *best,
+                             double *best_ms, int *from_cache);
+
 /* ---- serving loop (continuous batching of render requests over resident scenes) ----------- */
 
 /* Wave policies of the serving loop. */

@@ -108,6 +108,19 @@ class BatchTuneResult(C.Structure):
     _fields_ = [("tuning", BatchTuning), ("ms", C.c_float)]
 
 
+class TuningClass(C.Structure):
+    """pt_tuning_class: the device and the bucketed scale of a batch a cached tuning is reused for."""
+    _fields_ = [("device", C.c_char * 64), ("sm_count", C.c_uint32), ("compute_capability", C.c_uint32),
+                ("items_log2", C.c_uint32), ("pixels_log2", C.c_uint32), ("samples_log2", C.c_uint32),
+                ("faces_log2", C.c_uint32), ("tree_depth", C.c_uint32), ("max_depth", C.c_uint32),
+                ("flags", C.c_uint32)]
+
+    def as_dict(self):
+        d = {k: int(getattr(self, k)) for k, _ in self._fields_[1:]}
+        d["device"] = bytes(self.device).split(b"\0", 1)[0].decode("utf-8", errors="replace")
+        return d
+
+
 class ServerConfig(C.Structure):
     _fields_ = [("max_inflight", C.c_uint32), ("memory_budget", C.c_uint64), ("wave_pixels", C.c_uint64),
                 ("tuning", BatchTuning), ("policy", C.c_uint32), ("host_budget", C.c_uint64)]
@@ -173,6 +186,12 @@ def _load() -> C.CDLL:
         "pt_batch_destroy": (i, [_vp]),
         "pt_batch_autotune": (i, [C.POINTER(BatchItem), u32, C.POINTER(BatchTuning), C.POINTER(C.c_double),
                                   C.POINTER(BatchTuneResult), C.POINTER(u32)]),
+        "pt_tuning_class_of": (i, [C.POINTER(BatchItem), u32, C.POINTER(TuningClass)]),
+        "pt_tuning_cache_get": (i, [C.c_char_p, C.POINTER(TuningClass), C.POINTER(BatchTuning), C.POINTER(C.c_double),
+                                    C.POINTER(i)]),
+        "pt_tuning_cache_put": (i, [C.c_char_p, C.POINTER(TuningClass), C.POINTER(BatchTuning), C.c_double]),
+        "pt_batch_autotune_cached": (i, [C.POINTER(BatchItem), u32, C.c_char_p, C.POINTER(BatchTuning),
+                                         C.POINTER(C.c_double), C.POINTER(i)]),
         "pt_server_create": (i, [C.POINTER(ServerConfig), C.POINTER(_vp)]),
         "pt_server_submit": (i, [_vp, _vp, C.POINTER(RenderDesc), C.POINTER(u64)]),
         "pt_server_poll": (i, [_vp, u64, C.POINTER(i), C.POINTER(C.c_double)]),
@@ -605,6 +624,36 @@ def autotune(jobs, max_results: int = 64):
     check(lib.pt_batch_autotune(items, len(jobs), C.byref(best), C.byref(ms), res, C.byref(n)))
     trials = [(res[k].tuning.as_dict(), float(res[k].ms)) for k in range(n.value)]
     return best, float(ms.value), trials
+
+
+def tuning_class(jobs) -> TuningClass:
+    """The class (device and bucketed scale) of a batch, the key of the tuning cache."""
+    jobs = list(jobs)
+    cls = TuningClass()
+    check(lib.pt_tuning_class_of(_batch_items(jobs), len(jobs), C.byref(cls)))
+    return cls
+
+
+def tuning_cache_get(path, cls: TuningClass):
+    """(tuning, ms) stored for the class in the JSON cache file, or None."""
+    t, ms, found = BatchTuning(), C.c_double(0), C.c_int(0)
+    check(lib.pt_tuning_cache_get(os.fsencode(path), C.byref(cls), C.byref(t), C.byref(ms), C.byref(found)))
+    return (t, float(ms.value)) if found.value else None
+
+
+def tuning_cache_put(path, cls: TuningClass, tuning: BatchTuning, ms: float) -> None:
+    """Store (or replace) the class's tuning in the JSON cache file."""
+    check(lib.pt_tuning_cache_put(os.fsencode(path), C.byref(cls), C.byref(tuning), float(ms)))
+
+
+def autotune_cached(jobs, path):
+    """pt_batch_autotune_cached: (best tuning, ms, True) from the cache file when the batch's class
+    is there, else the search's (best, ms, False), stored in the file before return."""
+    jobs = list(jobs)
+    best, ms, hit = BatchTuning(), C.c_double(0), C.c_int(0)
+    check(lib.pt_batch_autotune_cached(_batch_items(jobs), len(jobs), os.fsencode(path), C.byref(best), C.byref(ms),
+                                       C.byref(hit)))
+    return best, float(ms.value), bool(hit.value)
 
 
 # ---- serving loop ---------------------------------------------------------------------------
