@@ -609,7 +609,7 @@ def main():
             line["batched"] = bench_batched(pb, torch)
         if not args.no_render and world == 1:
             line["render"] = bench_render(pb, torch, cpu=not args.no_cpu_baseline)
-        if not args.no_cpu_baseline:
+        if not args.no_cpu_baseline and world == 1:  # the host baseline is an N=1 figure
             threads = os.cpu_count() or 1
             v, kind, dt = cpu_reference(meshes, rays, args.ref_sample, threads)
             line["cpu_baseline"] = {"value": round(v, 4), "unit": "Mrays/s", "cores": threads, "kind": kind,
