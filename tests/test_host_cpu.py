@@ -288,3 +288,28 @@ def test_png_quantisation_oracle_known_answers():
     rgb = np.array([[[0.0, 0.5, 254.99], [255.0, 300.0, 1e9], [1.0, 127.9999, 128.0]]], np.float32)
     exp = np.array([[[0, 0, 254, 255], [255, 255, 255, 255], [1, 127, 128, 255]]], np.uint8)
     assert np.array_equal(po.film_to_rgba8(rgb), exp)
+
+
+def test_nan_inf_and_signed_zero_geometry_builds_deterministically():
+    """Faces with NaN or infinite coordinates (which the reference's bucket index cannot handle:
+    its unsigned conversion of a NaN is undefined) and coordinates of both zero signs: the build
+    stays in bounds, gives the same bytes for every thread count, and lists every face once."""
+    rng = np.random.default_rng(11)
+    nf = 150_000
+    v = rng.normal(size=(3 * nf, 3)).astype(np.float32)
+    v[rng.integers(0, len(v), 200), rng.integers(0, 3, 200)] = np.nan
+    v[rng.integers(0, len(v), 50), rng.integers(0, 3, 50)] = np.inf
+    v[rng.integers(0, len(v), 50), rng.integers(0, 3, 50)] = -np.inf
+    z = rng.integers(0, len(v), 5000)
+    v[z, rng.integers(0, 3, 5000)] = np.where(rng.random(5000) < 0.5, np.float32(0.0), np.float32(-0.0))
+    meshes = [pb.Mesh(v[:, 0], v[:, 1], v[:, 2], np.arange(3 * nf, dtype=np.uint32).reshape(-1, 3)),
+              pb.Mesh(v[::-1, 0].copy(), v[::-1, 1].copy(), v[::-1, 2].copy(),
+                      np.arange(3 * nf, dtype=np.uint32).reshape(-1, 3)[:40_000])]
+    ref_nodes, ref_pairs = pb.bvh_build(meshes, threads=1)
+    for threads in (0, 3, 16):
+        nodes, pairs = pb.bvh_build(meshes, threads=threads)
+        assert nodes.tobytes() == ref_nodes.tobytes() and pairs.tobytes() == ref_pairs.tobytes()
+    ids = ref_pairs[:, 0].astype(np.int64) * (1 << 32) + ref_pairs[:, 1]
+    assert len(np.unique(ids)) == nf + 40_000
+    leaves = ref_nodes[ref_nodes["num_faces"] > 0]
+    assert int(leaves["num_faces"].sum()) == nf + 40_000
