@@ -274,3 +274,24 @@ def test_mutated_files_fail_cleanly(tmp_path):
         except pb.PolytopeError as e:
             assert e.code in (pb.PT_EINVAL, pb.PT_ENOMEM)
     (tmp_path / "scene.pbrt").write_bytes(seeds["pbrt"])
+
+
+SPACING = ["[ 40 ]", "[40]", "40", "[ 40]", "[40 ]"]
+ARRAYS = ["[.6 .5 .4]", "[ .6 .5 .4 ]", "[ .6 .5 .4]", "[.6 .5 .4 ]"]
+
+
+@pytest.mark.parametrize("fov", SPACING)
+@pytest.mark.parametrize("kd", ARRAYS)
+def test_bracket_spacing_variants(tmp_path, fov, kd):
+    """The reference's scanner tests (tests/parsers/pbrt/test_scan.cpp:49-104: single values in
+    brackets with and without spaces or without brackets, arrays with and without inner spaces)
+    restated on whole files: every spelling reads the same, and the same as the reference parser."""
+    write_assets(tmp_path)
+    path = tmp_path / "s.pbrt"
+    path.write_text(f'LookAt 0 0 5  0 0 0  0 1 0\nCamera "perspective" "float fov" {fov}\nWorldBegin\n'
+                    f'Material "matte" "rgb Kd" {kd}\nShape "plymesh" "string filename" [ "quad.ply" ]\nWorldEnd\n')
+    s = pb.load_pbrt(path)
+    assert np.float32(s.camera["fov"]) == np.float32(40)
+    assert np.array_equal(np.float32(s.meshes[0].albedo), np.float32([.6, .5, .4]))
+    if po.ref_available():
+        assert_same_as_reference(s, po.ref_load_pbrt(str(path)))
