@@ -223,6 +223,12 @@ def test_defaults_and_identity_camera(tmp_path):
     ('LookAt 0 0 5 0 0 0 0 1 0\nWorldBegin\nShape "plymesh" "string filename" [ "missing.ply" ]\nWorldEnd\n', "missing"),
     ('LookAt 0 0 5 0 0 0 0 1 0\nWorldBegin\nWorldEn\n', "WorldEn"),
     ('LookAt 0 0 5 0 0 0 0 1 0\nCamera "perspective" "float fov [ 30 ]\n', "unterminated"),
+    # the reference's lexer tests ScaleDirective2 / ScaleDirective3 (tests/parsers/pbrt/test_lex.cpp:54-62)
+    # expect its process to exit with status 1 for these; the reader returns PT_EINVAL instead
+    ('LookAt 0 0 5 0 0 0 0 1 0\nWorldBegin\nScale 1 2\nWorldEnd\n', "Scale takes 3 numbers"),
+    ('LookAt 0 0 5 0 0 0 0 1 0\nWorldBegin\nScale 1 2 3 4\nWorldEnd\n', "Scale takes 3 numbers"),
+    ('LookAt 0 0 5 0 0 0 0 1 0\nWorldBegin\nTranslate 1 2\nWorldEnd\n', "Translate takes 3 numbers"),
+    ('LookAt 0 0 5 0 0 0 0 1 0\nWorldBegin\nRotate 30 0 1\nWorldEnd\n', "Rotate takes 4 numbers"),
 ])
 def test_unsupported_or_malformed_files_are_rejected(tmp_path, text, why):
     (tmp_path / "bad.pbrt").write_text(text)
