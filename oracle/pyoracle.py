@@ -324,6 +324,31 @@ def film_to_rgba8(rgb: np.ndarray) -> np.ndarray:
     return out
 
 
+def ref_png_film(rgb: np.ndarray, path) -> None:
+    """The reference's PNGFilm::Output (oracle/_ref): a float film (H, W, 3) through a BoxFilter of
+    one sample per pixel, quantised and encoded with lodepng into `path`."""
+    rgb = np.ascontiguousarray(rgb, np.float32)
+    h, w = rgb.shape[:2]
+    f = ref_lib().ref_png_film
+    f.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_char_p]
+    f.restype = None
+    f(rgb.ctypes.data, w, h, os.fsencode(str(path)))
+
+
+def ref_png_decode(path) -> np.ndarray:
+    """A PNG file decoded by the reference's lodepng (oracle/_ref): (H, W, 4) uint8."""
+    f = ref_lib().ref_png_decode
+    f.argtypes = [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_void_p, C.c_size_t]
+    f.restype = C.c_uint
+    w, h = C.c_uint32(), C.c_uint32()
+    cap = 1 << 26
+    buf = np.zeros(cap, np.uint8)
+    err = f(os.fsencode(str(path)), C.byref(w), C.byref(h), buf.ctypes.data, cap)
+    if err:
+        raise ValueError(f"lodepng error {err}")
+    return buf[:w.value * h.value * 4].reshape(h.value, w.value, 4).copy()
+
+
 def ref_load_ply(path: str):
     """The reference's own ply_parser::parse_file (oracle/_ref): (x, y, z, faces, normals or None)."""
     lib = ref_lib()

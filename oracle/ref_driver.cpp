@@ -38,6 +38,9 @@
 #include "cpu/cameras/PerspectiveCamera.h"
 #include "cpu/shading/brdf/mirror_brdf.h"
 #include "cpu/structures/stats.h"
+#include "cpu/films/PNGFilm.h"
+#include "cpu/filters/BoxFilter.h"
+#include "../lib/lodepng.h"  // lodepng, beside the reference sources (REF/lib)
 
 // Globals the reference translation units expect (defined by src/cpu/main.cpp in the reference).
 poly::Logger Log;
@@ -639,6 +642,38 @@ void ref_pbrt_mesh(void* h, uint32_t i, uint32_t* u, float* f, float* x, float* 
         std::memcpy(ny, g.ny_packed.data(), 4 * g.ny_packed.size());
         std::memcpy(nz, g.nz_packed.data(), 4 * g.nz_packed.size());
     }
+}
+
+
+// ---- the reference's film output (PNGFilm.cpp:20-58) and its PNG library, for the output tests ----
+// ref_png_film writes a float film (width*height*3, row-major) the way the reference's render call
+// ends: each pixel enters a BoxFilter as one sample at its centre, then PNGFilm::Output quantises
+// and encodes with lodepng.  A film the reference cannot encode ends the process (ERROR exits).
+void ref_png_film(const float* rgb, uint32_t width, uint32_t height, const char* path) {
+    const poly::Bounds bounds(width, height);
+    auto filter = std::make_unique<poly::BoxFilter>(bounds);
+    filter->SetSamples(1);
+    poly::PNGFilm film(bounds, path, std::move(filter));
+    for (uint32_t y = 0; y < height; ++y)
+        for (uint32_t x = 0; x < width; ++x) {
+            const float* p = rgb + 3 * ((size_t)y * width + x);
+            film.AddSample(poly::Point2f((float)x + 0.5f, (float)y + 0.5f),
+                           poly::Sample(poly::SpectralPowerDistribution(p[0], p[1], p[2])));
+        }
+    film.Output();
+}
+
+// lodepng's decoder: a PNG file as RGBA8.  Returns lodepng's error code (0 = ok); *w and *h are
+// set on success, and rgba receives min(cap, w*h*4) bytes.
+unsigned ref_png_decode(const char* path, uint32_t* w, uint32_t* h, uint8_t* rgba, size_t cap) {
+    std::vector<unsigned char> out;
+    unsigned ww = 0, hh = 0;
+    const unsigned err = lodepng::decode(out, ww, hh, std::string(path));
+    if (err) return err;
+    *w = ww;
+    *h = hh;
+    std::memcpy(rgba, out.data(), std::min(cap, out.size()));
+    return 0;
 }
 
 }  // extern "C"

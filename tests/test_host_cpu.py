@@ -313,3 +313,20 @@ def test_nan_inf_and_signed_zero_geometry_builds_deterministically():
     assert len(np.unique(ids)) == nf + 40_000
     leaves = ref_nodes[ref_nodes["num_faces"] > 0]
     assert int(leaves["num_faces"].sum()) == nf + 40_000
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="oracle/_ref is only built where the reference tree is present")
+@pytest.mark.parametrize("w,h", [(1, 1), (37, 5), (160, 120)])
+def test_png_output_matches_the_reference_film_output(tmp_path, w, h):
+    """The output step against the reference's own: a float film written by PNGFilm::Output
+    (BoxFilter of one sample per pixel, clamp and truncation, lodepng encoding) and the same film
+    quantised by the restatement and written by pt_write_png decode, with the reference's lodepng,
+    to the same RGBA8 pixels (the GPU tests pin pt_film_to_rgba8 to the restatement)."""
+    rng = np.random.default_rng(w * 31 + h)
+    rgb = rng.uniform(0, 400, (h, w, 3)).astype(np.float32)  # films are >= 0 (negative casts are undefined in C++)
+    rgb[0, 0] = (255.0, 254.99998, 0.0)
+    po.ref_png_film(rgb, tmp_path / "ref.png")
+    pb.write_png(tmp_path / "ours.png", po.film_to_rgba8(rgb))
+    want = po.ref_png_decode(tmp_path / "ref.png")
+    got = po.ref_png_decode(tmp_path / "ours.png")
+    assert want.shape == (h, w, 4) and np.array_equal(got, want)
