@@ -7,9 +7,10 @@
 //
 // What runs here is the reference's code: poly::bvh::bound / compact / intersect_compact,
 // poly::Mesh::intersect, poly::BoundingBox::Hits, poly::Transform, poly::PerspectiveCamera,
-// poly::Intersection::WorldToLocal / LocalToWorld, poly::MirrorBRDF::sample and the spectrum
-// types.  The only code of this file's own is the glue and the render-loop patches that the
-// reference cannot run as shipped (its RNG is seeded from std::random_device, constants.h:86-104):
+// poly::Intersection::WorldToLocal / LocalToWorld, poly::MirrorBRDF::sample, the spectrum types,
+// the PLY / OBJ / PBRT parsers, and PNGFilm::Output with BoxFilter and lodepng.  The only code of
+// this file's own is the glue and the render-loop patches that the reference cannot run as shipped
+// (its RNG is seeded from std::random_device, constants.h:86-104):
 //   P1 counter-based RNG (Philox4x32-10) keyed (pixel, sample, bounce); portable sin/cos of 2*pi*u
 //   P2 the post-hit frame comes from the mesh that owns the hit face: the hit face is re-tested
 //      alone on its own mesh (poly::Mesh::intersect with MinT = +inf), which recomputes the commit
