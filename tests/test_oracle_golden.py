@@ -339,3 +339,18 @@ def test_oracle_matches_reference_with_vertex_normals(tmp_path):
     assert_bit_equal(a, b, "film")
     assert_bit_equal(pa, pb_, "primary ids")
     assert a.mean() > 0.5
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="oracle/_ref is only built where the reference tree is present")
+@pytest.mark.parametrize("w,h,spp,depth", [(1, 1, 1, 0), (7, 3, 2, 1), (13, 9, 3, 2), (2, 17, 1, 9)])
+@pytest.mark.parametrize("flags", [0, 1, 3], ids=["bsdf", "nee", "nee_jitter"])
+def test_oracle_matches_reference_on_edge_render_shapes(w, h, spp, depth, flags):
+    """Degenerate frame shapes and depths (one pixel, odd sizes, max depth 0 and 1, a deeper path
+    than the configurations use): films and primary ids equal the reference's render loop."""
+    meshes, env = W.small_scene(level=3)
+    o, r = po.OracleScene(meshes, env), po.RefScene(meshes, env)
+    d = dict(width=w, height=h, spp=spp, max_depth=depth, seed=17, camera=W.SMALL_CAMERA, flags=flags)
+    a, pa = o.render(d)
+    b, pb_ = r.render(d)
+    assert_bit_equal(a, b, "film")
+    assert_bit_equal(pa, pb_, "primary ids")
