@@ -354,3 +354,36 @@ def test_oracle_matches_reference_on_edge_render_shapes(w, h, spp, depth, flags)
     b, pb_ = r.render(d)
     assert_bit_equal(a, b, "film")
     assert_bit_equal(pa, pb_, "primary ids")
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="oracle/_ref is only built where the reference tree is present")
+def test_oracle_matches_reference_on_edge_rays():
+    """The edge-case ray set of the device tests (both windings, axis-aligned directions with
+    infinite inverses, rays through edges and vertices, tmax 0 and just short of the hit, origins
+    inside boxes) plus directions with signed zeros: closest hits and per-ray counts equal the
+    reference's bvh::intersect_compact, and any-hit outcomes equal its closest-hit predicate."""
+    v = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1], [1, 1, 1]], np.float32)
+    meshes = [pb.Mesh(v[:, 0], v[:, 1], v[:, 2], np.array([[0, 1, 2], [0, 2, 1], [1, 3, 4], [0, 3, 1]], np.uint32))]
+    cases = []
+    for o, d in [((0.25, 0.25, 5), (0, 0, -1)), ((0.25, 0.25, -5), (0, 0, 1)), ((0.5, 0, 5), (0, 0, -1)),
+                 ((0, 0, 5), (0, 0, -1)), ((0.5, 0.5, 5), (0, 0, -1)), ((1, 0, 5), (0, 0, -1)),
+                 ((0.3, 0.3, 0.1), (0, 0, -1)), ((0.2, 0.2, 0.2), (1, 0, 0)), ((-1, 0.5, 0.5), (1, 0, 0)),
+                 ((0.5, 0.5, 0.5), (0, 1, 0)), ((0.25, 0.25, 5), (0, 0, 1)), ((2, 2, 2), (-1, -1, -1)),
+                 ((0.25, 0.25, 5), (-0.0, 0.0, -1)), ((0.25, 0.25, 5), (0.0, -0.0, -1)),
+                 ((0.5, 0.5, -2), (-0.0, -0.0, 1)), ((1, 1, 1), (-0.57735026, -0.57735026, -0.57735026))]:
+        for tmax in (np.inf, 0.0, 4.9999, 5.0):
+            for flags in (0, 1):
+                cases.append((o, d, tmax, flags))
+    rays = np.zeros(len(cases), po.RAY_DTYPE)
+    for i, (o, d, tmax, flags) in enumerate(cases):
+        rays["org"][i], rays["dir"][i], rays["tmax"][i], rays["flags"][i] = o, d, tmax, flags
+    o_, r_ = po.OracleScene(meshes), po.RefScene(meshes)
+    ho, nto, tto = o_.trace(rays, counts=True)
+    hr, ntr, ttr = r_.trace(rays, counts=True)
+    c = rays["flags"] == 0
+    for f in ("prim", "t", "u", "v"):
+        assert_bit_equal(ho[f][c], hr[f][c], f)
+    assert_bit_equal(nto[c], ntr[c], "nodes")
+    assert_bit_equal(tto[c], ttr[c], "faces")
+    assert ((ho["prim"] != po.PRIM_NONE) == (hr["prim"] != po.PRIM_NONE)).all()
+    assert (ho["prim"][c] != po.PRIM_NONE).sum() >= 10
