@@ -1,7 +1,7 @@
 """The C ABI from C and C++ callers: include/polytope_b200.h compiles as C99 and as C++17, and a
-program linked against the library reads a PBRT scene, its meshes and a PLY file and builds the
-reference tree through the exported entry points (calls that need no GPU), with the same results as
-the Python binding."""
+program linked against the library reads a PBRT scene, its meshes and a PLY file, builds the
+reference tree and round-trips a tuning-cache entry through the exported entry points (calls that
+need no GPU), with the same results as the Python binding."""
 import os
 import shutil
 import subprocess
@@ -42,6 +42,19 @@ int main(int argc, char **argv) {
     if (pt_load_ply(argv[2], &ply) != PT_OK) { printf("error %s\n", pt_last_error()); return 1; }
     printf("%u %u %d\n", ply.num_vertices, ply.num_faces, ply.nx != NULL);
     pt_mesh_data_free(&ply);
+    pt_tuning_class cls = {0};
+    snprintf(cls.device, sizeof cls.device, "%s", "C caller GPU");
+    cls.sm_count = 148;
+    cls.compute_capability = 100;
+    cls.items_log2 = 3;
+    pt_batch_tuning t, back;
+    pt_batch_default_tuning(&t);
+    t.queue_chunk = 96;
+    double ms = 0;
+    int found = 0;
+    const int put = pt_tuning_cache_put(argv[3], &cls, &t, 2.5);
+    const int get = pt_tuning_cache_get(argv[3], &cls, &back, &ms, &found);
+    printf("%d %d %d %.3g %u\n", put, get, found, ms, back.queue_chunk);
     printf("%s\n", pt_version());
     return 0;
 }
@@ -67,7 +80,7 @@ def test_c_and_cpp_callers(tmp_path, compiler, std):
     if not shutil.which(compiler):
         pytest.skip(f"{compiler} not available")
     scene = write_scene(tmp_path)
-    lines = build_and_run(tmp_path, compiler, std, "caller", [scene, tmp_path / "blob.ply"])
+    lines = build_and_run(tmp_path, compiler, std, "caller", [scene, tmp_path / "blob.ply", tmp_path / "tune.json"])
     s = pb.load_pbrt(scene)
     nodes, pairs = pb.bvh_build(s.meshes)
     faces = sum(len(m.faces) for m in s.meshes)
@@ -77,7 +90,8 @@ def test_c_and_cpp_callers(tmp_path, compiler, std):
     assert int(f[8]) == len(nodes) and int(f[9]) == int(nodes[0]["offset"])
     m = pb.load_ply(tmp_path / "blob.ply")
     assert lines[1].split() == [str(len(m.x)), str(len(m.faces)), "1"]
-    assert lines[2] == pb.version()
+    assert lines[2].split() == ["0", "0", "1", "2.5", "96"]  # the tuning cache from C
+    assert lines[3] == pb.version()
 
 
 def test_render_example_builds_and_fails_cleanly_without_a_device(tmp_path):
