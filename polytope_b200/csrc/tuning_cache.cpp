@@ -17,9 +17,9 @@
 #include <unistd.h>
 
 #include <cerrno>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
-#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <set>
@@ -150,8 +150,10 @@ private:
             if (p_ >= end_ || !(*p_ >= '0' && *p_ <= '9')) return err("bad number");
             while (p_ < end_ && *p_ >= '0' && *p_ <= '9') ++p_;
         }
-        const std::string text(s, p_);
-        v = std::strtod(text.c_str(), nullptr);
+        // from_chars, unlike strtod, ignores the process locale (a decimal comma would cut "1.5")
+        const std::from_chars_result r = std::from_chars(s, p_, v);
+        if (r.ec == std::errc::result_out_of_range) return err("number out of range");
+        if (r.ec != std::errc() || r.ptr != p_) return err("bad number");
         return true;
     }
     bool value(Json& v, int depth) {
@@ -312,8 +314,11 @@ std::string to_json(const std::vector<Entry>& entries) {
             std::snprintf(b, sizeof(b), ", \"%s\": %u", f.name, (unsigned)(e.tuning.*(f.member)));
             o += b;
         }
-        std::snprintf(b, sizeof(b), "}, \"ms\": %.17g}", e.ms);
-        o += b;
+        // the shortest text that reads back to the same double, whatever the process locale
+        o += "}, \"ms\": ";
+        const std::to_chars_result r = std::to_chars(b, b + sizeof(b), e.ms);
+        o.append(b, r.ptr);
+        o += '}';
     }
     o += entries.empty() ? "]}\n" : "\n]}\n";
     return o;
@@ -434,7 +439,8 @@ extern "C" int pt_tuning_class_of(const pt_batch_item* items, uint32_t n, pt_tun
     cudaDeviceProp p;
     const cudaError_t e = cudaGetDeviceProperties(&p, items[0].scene->device);
     if (e != cudaSuccess) return fail(PT_ECUDA, std::string("cudaGetDeviceProperties: ") + cudaGetErrorString(e));
-    std::strncpy(c.device, p.name, sizeof(c.device) - 1);
+    const size_t name_len = std::min(strnlen(p.name, sizeof(p.name)), sizeof(c.device) - 1);
+    std::memcpy(c.device, p.name, name_len);  // c.device is zeroed, so the name stays terminated
     c.sm_count = (uint32_t)p.multiProcessorCount;
     c.compute_capability = (uint32_t)(p.major * 10 + p.minor);
     *cls = c;
