@@ -387,3 +387,23 @@ def test_oracle_matches_reference_on_edge_rays():
     assert_bit_equal(tto[c], ttr[c], "faces")
     assert ((ho["prim"] != po.PRIM_NONE) == (hr["prim"] != po.PRIM_NONE)).all()
     assert (ho["prim"][c] != po.PRIM_NONE).sum() >= 10
+
+
+@pytest.mark.skipif(not po.ref_available(), reason="oracle/_ref is only built where the reference tree is present")
+def test_oracle_matches_reference_on_serving_pool_scenes():
+    """The two smallest of the first four resident scenes of the serving workload (the displaced
+    sphere instanced with seeded rigid transforms, Lambert or mirror, over a ground quad, a 3x3
+    light and environment 0.2): trees byte for byte, and an 8-row band of a 256x256, 4 spp, depth 5
+    request with NEE renders identically."""
+    pool = sorted(W.serving_pool(4), key=lambda s: sum(len(m.faces) for m in s[0]))[:2]
+    for meshes, env in pool:
+        o, r = po.OracleScene(meshes, env), po.RefScene(meshes, env)
+        no, po_ = o.tree()
+        nr, pr = r.tree()
+        assert no.tobytes() == nr.tobytes() and (po_ == pr).all()
+        d = dict(width=256, height=256, spp=4, max_depth=5, seed=23, camera=W.SERVE_CAMERA, flags=1)
+        a, pa = o.render(d, rows=(124, 132))
+        b, pb_ = r.render(d, rows=(124, 132))
+        assert_bit_equal(a, b, "band film")
+        assert_bit_equal(pa, pb_, "band primary ids")
+        assert a[124:132].mean() > 0.1
