@@ -194,10 +194,11 @@ typedef struct pt_camera {
 #define PT_RENDER_NEE        1u   /* area-light next-event estimation with shadow rays       */
 #define PT_RENDER_JITTER     2u   /* jittered pixel samples (default: pixel centres, the
                                      reference CenterSampler, samplers.cpp:13-18)             */
-#define PT_RENDER_WAVEFRONT  4u   /* queue-based wavefront kernels (default: one fused path
-                                     kernel per wave)                                         */
+#define PT_RENDER_WAVEFRONT  4u   /* queue-based wavefront kernels                             */
 #define PT_RENDER_PERSISTENT 8u   /* one persistent path kernel per wave whose lanes take the
-                                     next path as soon as theirs ends (no PT_RENDER_WAVEFRONT) */
+                                     next path as soon as theirs ends: the default pipeline     */
+#define PT_RENDER_FUSED     16u   /* one thread per path, one launch per wave (the simplest
+                                     form); the three pipeline flags exclude each other        */
 
 typedef struct pt_render_desc {
     uint32_t  width, height;
@@ -209,12 +210,28 @@ typedef struct pt_render_desc {
     pt_camera camera;
 } pt_render_desc;
 
-/* Render one frame.  rgb_out: width*height*3 floats, the box-filtered film (per-sample clamp to
- * 255 then the mean, BoxFilter.cpp:14-71) before PNG quantization.  primary_prim_out (optional):
- * width*height global primitive ids hit by sample 0's camera ray (PT_PRIM_NONE on a miss).
- * Pointers follow mem_flags; with host pointers the call returns when the film is on the host. */
+/* Render one frame (replaces AbstractRunner::Run on N threads + Output, src/cpu/main.cpp:187-220,
+ * AbstractRunner.cpp:11-31).  rgb_out: width*height*3 floats, the box-filtered film (per-sample
+ * clamp to 255 then the mean, BoxFilter.cpp:14-71) before PNG quantization.  primary_prim_out
+ * (optional): width*height global primitive ids hit by sample 0's camera ray (PT_PRIM_NONE on a
+ * miss).  Every pipeline gives the same film bit for bit; without a pipeline flag the persistent
+ * path kernel runs.  Pointers follow mem_flags:
+ *   - host pointers: the call returns when the film is on the host, and reports PT_ESTACK if one
+ *     of its own paths met a traversal guard;
+ *   - PT_MEM_DEVICE: the call only queues the work on `stream` (its temporaries return to a
+ *     stream-ordered pool behind it) and returns; a guard failure raises the scene's device flag,
+ *     which pt_scene_status reports. */
 int pt_render(pt_scene *scene, const pt_render_desc *desc, float *rgb_out,
               uint32_t *primary_prim_out, uint32_t mem_flags, void *stream);
+
+/* Waits for `stream`, then reports (PT_ESTACK) and clears the scene's device error flag: set when
+ * a kernel of an asynchronous call on this scene (pt_render or pt_trace with PT_MEM_DEVICE,
+ * pt_render_noalloc, pt_batch_run, served requests) met a traversal guard since the last report.
+ * Host-memory pt_render / pt_trace calls report their own guard failures and leave it alone.  The
+ * guards are a stack deeper than the host checked or a node index outside the tree; a scene built
+ * by pt_scene_create (which validates the tree) does not reach them.  No counterpart in the
+ * reference (its errors call exit, src/common/utilities/Common.h:13). */
+int pt_scene_status(pt_scene *scene, void *stream);
 
 /* Same render as pt_render, for callers that cannot allocate device memory during the call: an
  * application that owns the whole device-memory budget and forbids allocations after start-up,
@@ -223,10 +240,15 @@ int pt_render(pt_scene *scene, const pt_render_desc *desc, float *rgb_out,
  * fixed 6 MiB device array inside the library instead of being allocated per call.
  *   - rgb_dev (width*height*3 floats) and primary_dev (width*height ids, optional) are DEVICE
  *     pointers owned by the caller; the call is asynchronous on `stream`.
- *   - At most 262,144 pixels (e.g. 512x512) per frame and 262,144 paths per wave; larger frames
- *     are rejected with PT_EINVAL.  Only the fused pipeline (no PT_RENDER_WAVEFRONT).
+ *   - At most 262,144 pixels (e.g. 512x512) per frame and 262,144 paths per wave (larger frames
+ *     run in several waves); larger frames are rejected with PT_EINVAL.  It always runs the fused
+ *     pipeline: PT_RENDER_WAVEFRONT and PT_RENDER_PERSISTENT are rejected with PT_EINVAL.
+ *   - A traversal guard failure in its kernels raises the scene's device flag, like every
+ *     asynchronous call: pt_scene_status (after the frame) reports it.
  *   - The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
- *     that device current; make that first call before any stream capture.
+ *     that device current; make that first call before any stream capture.  The address is kept
+ *     for the life of the process, so cudaDeviceReset must not be called while the library is in
+ *     use (it would also free every scene).
  *   - Every call shares the array and it keeps the previous call's contents (the film sums are
  *     cleared at the start of each call): calls that overlap on the GPU (different streams, or
  *     different host threads) race and must be serialised by the caller.

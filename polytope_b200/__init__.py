@@ -31,7 +31,7 @@ PRIM_NONE = 0xFFFFFFFF
 MAT_LAMBERT, MAT_MIRROR = 1, 2
 RAY_ANY_HIT = 1
 MEM_DEVICE = 1
-RENDER_NEE, RENDER_JITTER, RENDER_WAVEFRONT, RENDER_PERSISTENT = 1, 2, 4, 8
+RENDER_NEE, RENDER_JITTER, RENDER_WAVEFRONT, RENDER_PERSISTENT, RENDER_FUSED = 1, 2, 4, 8, 16
 
 RAY_DTYPE = np.dtype([("org", "<f4", 3), ("tmax", "<f4"), ("dir", "<f4", 3), ("flags", "<u4")])
 HIT_DTYPE = np.dtype([("prim", "<u4"), ("t", "<f4"), ("u", "<f4"), ("v", "<f4")])
@@ -170,6 +170,7 @@ def _load() -> C.CDLL:
         "pt_scene_get_trace_tuning": (i, [_vp, C.POINTER(TraceTuning)]),
         "pt_trace_autotune": (i, [_vp, _vp, u64, _vp, C.POINTER(TraceTuning), C.POINTER(C.c_float)]),
         "pt_render_noalloc": (i, [_vp, C.POINTER(RenderDesc), _vp, _vp, _vp]),
+        "pt_scene_status": (i, [_vp, _vp]),
         "pt_film_to_rgba8": (i, [_vp, u32, u32, _vp, u32, _vp]),
         "pt_load_ply": (i, [C.c_char_p, C.POINTER(MeshData)]),
         "pt_load_obj": (i, [C.c_char_p, C.POINTER(MeshData)]),
@@ -375,6 +376,14 @@ class Scene:
             return hits, nt, tt
         check(lib.pt_trace(self.handle, _ptr(rays), n, _ptr(hits), flags, stream or None))
         return hits
+
+    def status(self, stream: int = 0) -> int:
+        """pt_scene_status: waits for `stream`, then returns (and clears) the scene's device error
+        status -- PT_OK, or PT_ESTACK when a kernel of an asynchronous call met a traversal guard."""
+        rc = lib.pt_scene_status(self.handle, stream or None)
+        if rc not in (PT_OK, PT_ESTACK):
+            check(rc)
+        return rc
 
     def set_trace_tuning(self, shared_stack: int, queue_chunk: int):
         check(lib.pt_scene_set_trace_tuning(self.handle, C.byref(TraceTuning(shared_stack, queue_chunk))))

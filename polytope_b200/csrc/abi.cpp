@@ -58,7 +58,7 @@ void free_scene(pt_scene* s) {
     if (!s) return;
     DeviceGuard g(s->device);
     void* bufs[] = {s->dev.nodes, s->dev.tris, s->dev.meshes, s->dev.prim_normals, s->dev.prim_tri,
-                    s->dev.light_tris, s->dev.light_cdf, s->dev_in, s->dev_out, s->err_flag, s->ray_counters};
+                    s->dev.light_tris, s->dev.light_cdf, s->dev_in, s->dev_out, s->err_flag, s->trace_err, s->ray_counters};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (s->pin_in) cudaFreeHost(s->pin_in);
@@ -92,7 +92,8 @@ int ensure_staging(pt_scene* s) {
     for (int i = 0; i < 3 * kSlots + 1; ++i)
         PT_CUDA(cudaEventCreateWithFlags((cudaEvent_t*)&s->events[i], cudaEventDisableTiming));
     const size_t in_b = kSlots * kChunkRays * sizeof(pt_ray), out_b = kSlots * kChunkRays * sizeof(pt_hit);
-    if (cudaMalloc(&s->dev_in, in_b) != cudaSuccess || cudaMalloc(&s->dev_out, out_b) != cudaSuccess)
+    if (cudaMalloc(&s->dev_in, in_b) != cudaSuccess || cudaMalloc(&s->dev_out, out_b) != cudaSuccess ||
+        cudaMalloc(&s->trace_err, sizeof(int)) != cudaSuccess)
         return fail(PT_ENOMEM, "cudaMalloc staging buffers");
     if (cudaMallocHost(&s->pin_in, in_b) != cudaSuccess || cudaMallocHost(&s->pin_out, out_b) != cudaSuccess)
         return fail(PT_ENOMEM, "cudaMallocHost staging buffers");
@@ -150,7 +151,8 @@ int scene_trace(pt_scene* s, const pt_ray* rays, uint64_t n, pt_hit* hits, uint3
     cudaEvent_t *ev_in = ev, *ev_k = ev + kSlots, *ev_out = ev + 2 * kSlots, dep = ev[3 * kSlots];
     PT_CUDA(cudaEventRecord(dep, (cudaStream_t)stream));
     for (int i = 0; i < 4; ++i) PT_CUDA(cudaStreamWaitEvent((cudaStream_t)s->streams[i], dep, 0));
-    PT_CUDA(cudaMemsetAsync(s->err_flag, 0, sizeof(int), h2d));  // before every copy-in, so before every kernel
+    a.err = (int*)s->trace_err;  // this call's own flag: the asynchronous calls raise err_flag
+    PT_CUDA(cudaMemsetAsync(s->trace_err, 0, sizeof(int), h2d));  // before every copy-in, so before every kernel
     const bool pin_rays = is_pinned(rays), pin_hits = is_pinned(hits);
     const bool counted = node_tests || tri_tests;
     uint32_t* dcounts = nullptr;
@@ -219,7 +221,7 @@ int scene_trace(pt_scene* s, const pt_ray* rays, uint64_t n, pt_hit* hits, uint3
         if (tri_tests) std::memcpy(tri_tests, tmp.data() + n, n * sizeof(uint32_t));
     }
     int err = 0;
-    PT_CUDA(cudaMemcpy(&err, s->err_flag, sizeof(int), cudaMemcpyDeviceToHost));
+    PT_CUDA(cudaMemcpy(&err, s->trace_err, sizeof(int), cudaMemcpyDeviceToHost));
     if (err) return fail(PT_ESTACK, "a ray exceeded the traversal stack (malformed or too deep tree)");
     return PT_OK;
 }

@@ -275,8 +275,8 @@ extern "C" int pt_batch_create(const pt_batch_item* items, uint32_t n, const pt_
     for (uint32_t i = 0; i < n; ++i) {
         rc = check_render_desc(items[i].scene, &items[i].desc);
         if (rc) return fail(rc, "batch item " + std::to_string(i) + ": " + pt_last_error());
-        if (items[i].desc.flags & (PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT))
-            return fail(PT_EINVAL, "batch items take the batch's pipeline (no PT_RENDER_WAVEFRONT / PT_RENDER_PERSISTENT)");
+        if (items[i].desc.flags & (PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT | PT_RENDER_FUSED))
+            return fail(PT_EINVAL, "batch items take the batch's pipeline (no PT_RENDER_WAVEFRONT / PERSISTENT / FUSED)");
         if (i && items[i].scene->device != items[0].scene->device) return fail(PT_EINVAL, "batch items on different devices");
         max_depth = std::max(max_depth, items[i].scene->max_depth);
         b->scenes.push_back(items[i].scene);

@@ -53,16 +53,70 @@ PT_HD T ldg(const T* p) {
     return *p;
 #endif
 }
+// L2 residency of the scene versus the ray stream.  A ray query reads its 32-B ray and writes its
+// 16-B hit once, while every ray re-reads the upper tree and many leaves; on the 1.3 M-face
+// microbench the 768 MiB of rays and hits per launch streamed through the same L2 as the 113 MB
+// tree and pushed its hit rate down to 69 %.  With PT_L2_HINTS >= 1 rays and hits are loaded and
+// stored cache-streaming (evict-first in L1 and L2); with PT_L2_HINTS >= 2 node and face loads
+// also carry an L2::evict_last cache-hint policy.  Both are per-instruction hints: no device,
+// context or stream attribute is set.
+#ifndef PT_L2_HINTS
+#define PT_L2_HINTS 2
+#endif
+
+#if defined(__CUDA_ARCH__) && PT_L2_HINTS >= 2
+__device__ __forceinline__ uint64_t l2_keep_policy() {
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+#endif
+
 // One 32-byte node record (two uint4) with a single 256-bit read-only load on the device; the
 // record must be 32-byte aligned (node arrays are cudaMalloc'd and nodes are 32 bytes).
 PT_HD void ldg_node(const uint4* p, uint4& a, uint4& b) {
-#ifdef __CUDA_ARCH__
+#if defined(__CUDA_ARCH__) && PT_L2_HINTS >= 2
+    asm("ld.global.nc.L2::cache_hint.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8], %9;"
+        : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
+        : "l"(p), "l"(l2_keep_policy()));
+#elif defined(__CUDA_ARCH__)
     asm("ld.global.nc.v8.u32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
         : "=r"(a.x), "=r"(a.y), "=r"(a.z), "=r"(a.w), "=r"(b.x), "=r"(b.y), "=r"(b.z), "=r"(b.w)
         : "l"(p));
 #else
     a = p[0];
     b = p[1];
+#endif
+}
+// One 16-byte part of a face record (read-only, kept in L2 like the nodes).
+PT_HD float4 ldg_face(const float4* p) {
+#if defined(__CUDA_ARCH__) && PT_L2_HINTS >= 2
+    float4 v;
+    asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "l"(p), "l"(l2_keep_policy()));
+    return v;
+#elif defined(__CUDA_ARCH__)
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+// Ray records read once and hit records written once: streamed past the caches.
+PT_HD float4 ld_stream(const float4* p) {
+#if defined(__CUDA_ARCH__) && PT_L2_HINTS >= 1
+    return __ldcs(p);
+#elif defined(__CUDA_ARCH__)
+    return __ldg(p);
+#else
+    return *p;
+#endif
+}
+PT_HD void st_stream(uint4* p, uint4 v) {
+#if defined(__CUDA_ARCH__) && PT_L2_HINTS >= 1
+    __stcs(p, v);
+#else
+    *p = v;
 #endif
 }
 PT_HD void raise_flag(int* flag) {

@@ -7,7 +7,8 @@
 // This entry point runs the same kernels with the scratch taken from a file-scope device array
 // instead, so the call itself allocates nothing.  Limits: at most kMaxPixels pixels per frame and
 // at most kMaxWavePaths paths per wave (6 MiB in total, held by every device that loads the
-// library until the process exits).
+// library until the process exits).  Like every asynchronous call it leaves guard failures of its
+// kernels in the scene's device flag, which pt_scene_status reports once the frame is done.
 
 #include <mutex>
 #include <string>
@@ -54,8 +55,9 @@ extern "C" int pt_render_noalloc(pt_scene* s, const pt_render_desc* desc, float*
     int rc = check_render_desc(s, desc);
     if (rc) return rc;
     if (!rgb_dev) return fail(PT_EINVAL, "rgb_dev is NULL");
-    if (desc->flags & PT_RENDER_WAVEFRONT)
-        return fail(PT_EINVAL, "pt_render_noalloc runs the fused path kernel only (PT_RENDER_WAVEFRONT not accepted)");
+    if (desc->flags & (PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT))
+        return fail(PT_EINVAL, "pt_render_noalloc runs the fused path kernel only (PT_RENDER_WAVEFRONT and "
+                               "PT_RENDER_PERSISTENT are not accepted)");
     const uint64_t npix64 = (uint64_t)desc->width * desc->height;
     if (npix64 > kMaxPixels)
         return fail(PT_EINVAL, "frame of " + std::to_string(npix64) + " pixels exceeds the pt_render_noalloc limit of " +

@@ -126,7 +126,11 @@ struct pt_scene {
     size_t staging_rays = 0;
     void* streams[4] = {};  // host-pointer traces: copies in, two kernel streams, copies out
     void* events[16] = {};
-    void* err_flag = nullptr;  // device int, set when a kernel hit a guard
+    // device ints set when a kernel hits a guard: err_flag by the asynchronous (device-memory)
+    // calls, cleared when pt_scene_status reports it; trace_err by the host-memory pt_trace call
+    // that holds staging_mu
+    void* err_flag = nullptr;
+    void* trace_err = nullptr;
     // ray counters of the persistent trace kernel: one per launch in flight, taken round-robin
     void* ray_counters = nullptr;
     std::atomic<uint32_t> counter_next{0};

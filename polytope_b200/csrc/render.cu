@@ -169,10 +169,11 @@ int check_render_desc(const pt_scene* s, const pt_render_desc* desc) {
     if ((uint64_t)desc->width * desc->height > (1u << 30)) return fail(PT_EINVAL, "frame too large");
     if ((uint64_t)desc->width * desc->height * desc->spp > (1ull << 40)) return fail(PT_EINVAL, "too many samples");
     if (desc->max_depth > 1024) return fail(PT_EINVAL, "max_depth above 1024");
-    if (desc->flags & ~(uint32_t)(PT_RENDER_NEE | PT_RENDER_JITTER | PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT))
+    if (desc->flags & ~(uint32_t)(PT_RENDER_NEE | PT_RENDER_JITTER | PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT | PT_RENDER_FUSED))
         return fail(PT_EINVAL, "unknown render flags");
-    if ((desc->flags & PT_RENDER_WAVEFRONT) && (desc->flags & PT_RENDER_PERSISTENT))
-        return fail(PT_EINVAL, "PT_RENDER_WAVEFRONT and PT_RENDER_PERSISTENT exclude each other");
+    const uint32_t pipes = desc->flags & (PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT | PT_RENDER_FUSED);
+    if (pipes & (pipes - 1))
+        return fail(PT_EINVAL, "PT_RENDER_WAVEFRONT, PT_RENDER_PERSISTENT and PT_RENDER_FUSED exclude each other");
     if ((int)s->max_depth + 2 > PT_TRAVERSAL_STACK) return fail(PT_ESTACK, "tree too deep for the traversal stack");
     return PT_OK;
 }
@@ -190,26 +191,38 @@ extern "C" int pt_render(pt_scene* s, const pt_render_desc* desc, float* rgb_out
     if (prev != s->device) cudaSetDevice(s->device);
     struct Restore { int d; ~Restore() { if (d >= 0) cudaSetDevice(d); } } restore{prev != s->device ? prev : -1};
 
-    const RenderParams p = render_params(s, desc);
-    // the wave engine runs both the queue-based kernels and the persistent path kernel
-    const bool persistent = (desc->flags & PT_RENDER_PERSISTENT) != 0;
-    const bool wavefront = (desc->flags & PT_RENDER_WAVEFRONT) != 0 || persistent;
+    const bool dev_out = (mem_flags & PT_MEM_DEVICE) != 0;
+    RenderParams p = render_params(s, desc);
+    // Pipelines: the persistent path kernel unless PT_RENDER_FUSED or PT_RENDER_WAVEFRONT is given
+    // (the wave engine runs both the queue-based kernels and the persistent path kernel).
+    const bool fused = (desc->flags & PT_RENDER_FUSED) != 0;
+    const bool persistent = !fused && (desc->flags & PT_RENDER_WAVEFRONT) == 0;
+    const bool wavefront = !fused;
     cudaStream_t st = (cudaStream_t)stream;
     const uint64_t total = npix64 * desc->spp;
-    uint32_t wave = desc->wave_paths ? desc->wave_paths : (wavefront ? (1u << 22) : (1u << 22));
-    if (wave > total) wave = (uint32_t)total;
+    // Default wave: 4 M paths for the fused and queue-based kernels (the queues cost ~140 B per
+    // path), 32 M for the persistent path kernel (12 B per path; longer waves shorten its tail).
+    uint64_t wave = desc->wave_paths ? desc->wave_paths : (persistent ? (1ull << 25) : (1ull << 22));
+    if (wave > total) wave = total;
     cudaMemPool_t pool = render_pool(s->device);
     DevBuf rad, film, rgb_dev, prim_dev, wsbuf, tables;
-    if ((!wavefront && !rad.alloc(12 * (size_t)wave, pool, st)) || !film.alloc(12 * (size_t)npix, pool, st))
+    // the film sums, then (host-memory calls) this call's own error flag
+    const size_t film_bytes = (12 * (size_t)npix + 15) & ~(size_t)15;
+    if ((!wavefront && !rad.alloc(12 * (size_t)wave, pool, st)) || !film.alloc(film_bytes + 16, pool, st))
         return fail(PT_ENOMEM, "device memory for the render buffers");
+    // A host-memory call waits for its frame and reports a guard failure of its own kernels; a
+    // device-memory call returns once the work is queued, and its kernels raise the scene's flag,
+    // which pt_scene_status reads.
+    int* call_err = (int*)((char*)film.p + film_bytes);
+    p.err = dev_out ? (int*)s->err_flag : call_err;
     WfState ws{};
     WfPlan plan;
     if (wavefront) {
-        if (!wsbuf.alloc(wf_state_bytes(wave, persistent), pool, st)) return fail(PT_ENOMEM, "device memory for the wavefront queues");
-        wf_state_carve(wsbuf.p, wave, ws, persistent);
+        if (!wsbuf.alloc(wf_state_bytes((uint32_t)wave, persistent), pool, st))
+            return fail(PT_ENOMEM, "device memory for the wavefront queues");
+        wf_state_carve(wsbuf.p, (uint32_t)wave, ws, persistent);
         wf_plan_all(plan, {npix}, {desc->spp}, {desc->max_depth}, wave);
     }
-    const bool dev_out = (mem_flags & PT_MEM_DEVICE) != 0;
     float* rgb_d = rgb_out;
     uint32_t* prim_d = primary_out;
     if (!dev_out) {
@@ -220,17 +233,17 @@ extern "C" int pt_render(pt_scene* s, const pt_render_desc* desc, float* rgb_out
             prim_d = (uint32_t*)prim_dev.p;
         }
     }
-    cudaError_t e = cudaMemsetAsync(film.p, 0, 12 * (size_t)npix, st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(s->err_flag, 0, sizeof(int), st);
+    cudaError_t e = cudaMemsetAsync(film.p, 0, film_bytes + 16, st);
     if (wavefront) {
-        // one item: device copies of its parameters and of the plan's tables
+        // one item: device copies of its parameters and of the plan's tables, staged in one
+        // host block and copied with one call
         const size_t pbytes = (sizeof(RenderParams) + 255) & ~(size_t)255;
         const size_t ibytes = (sizeof(WfItem) + 255) & ~(size_t)255;
         const size_t sbytes = ((sizeof(WfSegment) * plan.segments.size()) + 255) & ~(size_t)255;
         const size_t rbytes = ((sizeof(WfPixels) * plan.resolve.size()) + 255) & ~(size_t)255;
         const size_t fbytes = sizeof(WfPixels) * plan.finish.size();
-        if (!tables.alloc(pbytes + ibytes + sbytes + rbytes + fbytes, pool, st))
-            return fail(PT_ENOMEM, "device memory for the wavefront tables");
+        const size_t tbytes = pbytes + ibytes + sbytes + rbytes + fbytes;
+        if (!tables.alloc(tbytes, pool, st)) return fail(PT_ENOMEM, "device memory for the wavefront tables");
         char* tb = (char*)tables.p;
         RenderParams* d_params = (RenderParams*)tb;
         WfItem* d_item = (WfItem*)(tb + pbytes);
@@ -257,16 +270,33 @@ extern "C" int pt_render(pt_scene* s, const pt_render_desc* desc, float* rgb_out
         if (e == cudaSuccess) e = launch_finish_film((const float*)film.p, npix, desc->spp, rgb_d, st);
     }
     if (e != cudaSuccess) return fail(PT_ECUDA, std::string("render launch: ") + cudaGetErrorString(e));
-    if (!dev_out) {
-        e = cudaMemcpyAsync(rgb_out, rgb_d, 12 * (size_t)npix, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess && primary_out)
-            e = cudaMemcpyAsync(primary_out, prim_d, 4 * (size_t)npix, cudaMemcpyDeviceToHost, st);
-    }
-    // the temporaries are freed at scope exit: the stream must be done with them
+    // Device-memory output: the temporaries go back to the pool in stream order, so nothing here
+    // waits for the frame.
+    if (dev_out) return PT_OK;
+    int err = 0;
+    e = cudaMemcpyAsync(rgb_out, rgb_d, 12 * (size_t)npix, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && primary_out)
+        e = cudaMemcpyAsync(primary_out, prim_d, 4 * (size_t)npix, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&err, call_err, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail(PT_ECUDA, std::string("render: ") + cudaGetErrorString(e));
-    int err = 0;
-    cudaMemcpy(&err, s->err_flag, sizeof(int), cudaMemcpyDeviceToHost);
     if (err) return fail(PT_ESTACK, "a path exceeded the traversal stack");
+    return PT_OK;
+}
+
+extern "C" int pt_scene_status(pt_scene* s, void* stream) {
+    if (!s) return fail(PT_EINVAL, "scene is NULL");
+    int prev = -1;
+    cudaGetDevice(&prev);
+    if (prev != s->device) cudaSetDevice(s->device);
+    struct Restore { int d; ~Restore() { if (d >= 0) cudaSetDevice(d); } } restore{prev != s->device ? prev : -1};
+    cudaStream_t st = (cudaStream_t)stream;
+    int err = 0;
+    cudaError_t e = cudaMemcpyAsync(&err, s->err_flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess && err) e = cudaMemsetAsync(s->err_flag, 0, sizeof(int), st);
+    if (e == cudaSuccess && err) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(PT_ECUDA, std::string("scene status: ") + cudaGetErrorString(e));
+    if (err) return fail(PT_ESTACK, "a kernel on this scene exceeded the traversal stack or met a malformed tree");
     return PT_OK;
 }

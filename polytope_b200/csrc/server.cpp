@@ -533,8 +533,8 @@ extern "C" int pt_server_submit(pt_server* s, pt_scene* scene, const pt_render_d
     if (!s || !ticket) return fail(PT_EINVAL, "server or ticket is NULL");
     int rc = check_render_desc(scene, desc);
     if (rc) return rc;
-    if (desc->flags & (PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT))
-        return fail(PT_EINVAL, "served requests take the server's pipeline (no PT_RENDER_WAVEFRONT / PT_RENDER_PERSISTENT)");
+    if (desc->flags & (PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT | PT_RENDER_FUSED))
+        return fail(PT_EINVAL, "served requests take the server's pipeline (no PT_RENDER_WAVEFRONT / PERSISTENT / FUSED)");
     if (scene->device != s->device) return fail(PT_EINVAL, "scene lives on another device");
     if (!stack_cap_for(scene->max_depth, s->cfg.tuning.stack_depth)) return fail(PT_ESTACK, "tree too deep");
     std::unique_ptr<Request> r(new Request());

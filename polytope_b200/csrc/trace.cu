@@ -16,8 +16,8 @@ __global__ void __launch_bounds__(128) trace_kernel(const uint4* __restrict__ no
                                                     uint32_t* tri_tests, int* err) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const float4 r0 = __ldg(rays + 2 * i);
-    const float4 r1 = __ldg(rays + 2 * i + 1);
+    const float4 r0 = ld_stream(rays + 2 * i);
+    const float4 r1 = ld_stream(rays + 2 * i + 1);
     RayState rs;
     ray_setup(rs, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
     const bool any = (__float_as_uint(r1.w) & 1u) != 0;
@@ -31,7 +31,7 @@ __global__ void __launch_bounds__(128) trace_kernel(const uint4* __restrict__ no
         h.x = 0xFFFFFFFEu;
         atomicExch(err, 1);
     }
-    hits[i] = h;
+    st_stream(hits + i, h);
     if (COUNT) {
         if (node_tests) node_tests[i] = tr.nodes;
         if (tri_tests) tri_tests[i] = tr.tris;
@@ -80,8 +80,8 @@ __global__ void __launch_bounds__(128, 8) trace_persistent_kernel(const uint4* _
             const uint32_t rank = __popc(need & lt_mask);
             if (!active && rank < avail) {
                 idx = pool_next + rank;
-                const float4 r0 = __ldg(rays + 2 * idx);
-                const float4 r1 = __ldg(rays + 2 * idx + 1);
+                const float4 r0 = ld_stream(rays + 2 * idx);
+                const float4 r1 = ld_stream(rays + 2 * idx + 1);
                 walk_begin(k, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, r0.w, (__float_as_uint(r1.w) & 1u) != 0);
                 active = true;
             }
@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(128, 8) trace_persistent_kernel(const uint4* _
                 h.z = __float_as_uint(k.u);
                 h.w = __float_as_uint(k.v);
                 if (!ok) atomicExch(err, 1);
-                hits[idx] = h;
+                st_stream(hits + idx, h);
                 if (COUNT) {
                     if (node_tests) node_tests[idx] = k.nodes;
                     if (tri_tests) tri_tests[idx] = k.tris;

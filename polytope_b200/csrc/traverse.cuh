@@ -313,7 +313,7 @@ template <bool COUNT, int CAP, int SH>
 PT_HD void walk_leaf(RayWalkT<CAP, SH>& k, const float4* __restrict__ tris, uint32_t leaf_off, uint32_t leaf_n) {
     for (uint32_t j = 0; j < leaf_n; ++j) {
         const size_t ti = 3 * (size_t)(leaf_off + j);
-        const float4 q0 = ldg(tris + ti), q1 = ldg(tris + ti + 1), q2 = ldg(tris + ti + 2);
+        const float4 q0 = ldg_face(tris + ti), q1 = ldg_face(tris + ti + 1), q2 = ldg_face(tris + ti + 2);
         if (COUNT) k.tris++;
         float t, u, v, w;
         if (wald(k.r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, k.min_t, t, u, v, w)) {
@@ -366,7 +366,7 @@ PT_HD TraceResult traverse(const uint4* __restrict__ nodes, const float4* __rest
         if (nf > 0) {
             for (uint32_t k = 0; k < nf; ++k) {
                 const size_t ti = 3 * (size_t)(b.z + k);
-                const float4 q0 = ldg(tris + ti), q1 = ldg(tris + ti + 1), q2 = ldg(tris + ti + 2);
+                const float4 q0 = ldg_face(tris + ti), q1 = ldg_face(tris + ti + 1), q2 = ldg_face(tris + ti + 2);
                 if (COUNT) res.tris++;
                 float t, u, v, w;
                 if (wald(r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, min_t, t, u, v, w)) {

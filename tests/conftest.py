@@ -11,6 +11,26 @@ if ROOT not in sys.path:
 GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
+def reference_root():
+    """The reference's source tree, for the CPU tests that read its headers, scenes and unit-test
+    files: $POLYTOPE_REFERENCE, else the tree oracle/Makefile built oracle/_ref from (recorded in
+    oracle/_ref/ref_root.txt).  None when neither names an existing directory (those tests skip)."""
+    root = os.environ.get("POLYTOPE_REFERENCE")
+    if not root:
+        try:
+            with open(os.path.join(ROOT, "oracle", "_ref", "ref_root.txt")) as f:
+                root = f.read().strip()
+        except OSError:
+            return None
+    return root if root and os.path.isdir(root) else None
+
+
+def reference_path(*parts):
+    """A path inside the reference tree, or a path that does not exist when the tree is absent."""
+    root = reference_root()
+    return os.path.join(root, *parts) if root else os.path.join(ROOT, "_no_reference_tree", *parts)
+
+
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); parity tests of the CUDA path")
 

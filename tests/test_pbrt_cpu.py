@@ -9,11 +9,13 @@ import os
 import numpy as np
 import pytest
 
+from conftest import reference_path
+
 import polytope_b200 as pb
 from oracle import pyoracle as po
 from test_ply_cpu import write_ply
 
-REF_SCENES = "/root/reference/scenes"
+REF_SCENES = reference_path("scenes")
 # example scenes of the reference that it parses and whose geometry files it ships
 MATCHING = ["bunny/bunny.pbrt", "bvh-test/bvh-test.pbrt", "lighttest/lighttest.pbrt", "minimum.pbrt",
             "minimum-emptyworld.pbrt", "teapot/teapot.pbrt", "test/cuda/bvh-traversal.pbrt",

@@ -11,7 +11,7 @@ from test_pbrt_cpu import write_assets, write_scene
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("pipeline", [0, pb.RENDER_WAVEFRONT, pb.RENDER_PERSISTENT], ids=["fused", "wavefront", "persistent"])
+@pytest.mark.parametrize("pipeline", [pb.RENDER_FUSED, pb.RENDER_WAVEFRONT, pb.RENDER_PERSISTENT], ids=["fused", "wavefront", "persistent"])
 def test_pbrt_scene_renders_like_the_oracle(cuda_device, tmp_path, pipeline):
     s = pb.load_pbrt(write_scene(tmp_path))
     scene = pb.Scene(s.meshes, s.env)

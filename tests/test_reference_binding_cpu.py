@@ -12,10 +12,12 @@ import subprocess
 
 import pytest
 
+from conftest import reference_path
+
 from test_pbrt_cpu import MATCHING, REF_SCENES, write_scene
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_SRC = "/root/reference/src"
+REF_SRC = reference_path("src")
 REF_LIB = os.path.join(ROOT, "oracle", "_ref")
 LIBDIR = os.path.join(ROOT, "polytope_b200", "lib")
 

@@ -11,9 +11,11 @@ import shutil
 import numpy as np
 import pytest
 
+from conftest import reference_path
+
 import polytope_b200 as pb
 
-SCENES = "/root/reference/scenes"
+SCENES = reference_path("scenes")
 pytestmark = pytest.mark.skipif(not os.path.isdir(SCENES), reason="needs the reference's scenes/ tree")
 
 

@@ -23,7 +23,7 @@ def image_errors(a, b):
     return rel, np.abs(a - b).mean() / max(np.abs(b).mean(), 1e-30)
 
 
-PIPELINES = [0, pb.RENDER_WAVEFRONT, pb.RENDER_PERSISTENT]
+PIPELINES = [pb.RENDER_FUSED, pb.RENDER_WAVEFRONT, pb.RENDER_PERSISTENT]
 
 
 @pytest.mark.parametrize("pipeline", PIPELINES, ids=["fused", "wavefront", "persistent"])
@@ -82,7 +82,8 @@ def test_instanced_scene_matches_reference_fixture(cuda_device, pipeline):
 
 @pytest.mark.parametrize("flags", [pb.RENDER_JITTER | pb.RENDER_NEE, pb.RENDER_JITTER,
                                    pb.RENDER_JITTER | pb.RENDER_NEE | pb.RENDER_WAVEFRONT,
-                                   pb.RENDER_JITTER | pb.RENDER_NEE | pb.RENDER_PERSISTENT])
+                                   pb.RENDER_JITTER | pb.RENDER_NEE | pb.RENDER_PERSISTENT,
+                                   pb.RENDER_JITTER | pb.RENDER_NEE | pb.RENDER_FUSED])
 def test_jitter_and_small_waves(cuda_device, flags):
     meshes, env = W.small_scene(level=3)
     scene = pb.Scene(meshes, env)
@@ -99,9 +100,41 @@ def test_jitter_and_small_waves(cuda_device, flags):
 def test_pipeline_flags_exclude_each_other(cuda_device):
     meshes, env = W.small_scene(level=1)
     scene = pb.Scene(meshes, env)
-    with pytest.raises(pb.PolytopeError) as e:
-        pb.render(scene, 8, 8, 1, 2, W.SMALL_CAMERA, flags=pb.RENDER_WAVEFRONT | pb.RENDER_PERSISTENT)
-    assert e.value.code == pb.PT_EINVAL
+    for bad in (pb.RENDER_WAVEFRONT | pb.RENDER_PERSISTENT, pb.RENDER_FUSED | pb.RENDER_PERSISTENT,
+                pb.RENDER_FUSED | pb.RENDER_WAVEFRONT, 32):
+        with pytest.raises(pb.PolytopeError) as e:
+            pb.render(scene, 8, 8, 1, 2, W.SMALL_CAMERA, flags=bad)
+        assert e.value.code == pb.PT_EINVAL
+
+
+def test_device_memory_render_is_asynchronous_and_reports_through_scene_status(cuda_device):
+    """With PT_MEM_DEVICE pt_render only queues its kernels on the given stream (nothing in the call
+    waits for the frame); frames queued back to back on one stream and on a second stream equal the
+    host-memory renders, and pt_scene_status reports no guard failure afterwards."""
+    import ctypes as C
+    import torch
+    meshes, env = W.small_scene(level=3)
+    scene = pb.Scene(meshes, env)
+    frames = [(64, 48, 3, 1, pb.RENDER_NEE), (40, 30, 2, 5, pb.RENDER_NEE | pb.RENDER_JITTER),
+              (33, 17, 4, 9, pb.RENDER_NEE | pb.RENDER_FUSED), (50, 20, 2, 2, pb.RENDER_NEE | pb.RENDER_WAVEFRONT)]
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    outs = []
+    for k, (w, h, spp, seed, flags) in enumerate(frames):
+        rd = pb.render_desc(w, h, spp, 4, W.SMALL_CAMERA, seed, flags)
+        rgb = torch.full((w * h * 3,), float("nan"), dtype=torch.float32, device=cuda_device)
+        prim = torch.zeros(w * h, dtype=torch.int32, device=cuda_device)
+        st = streams[k % 2]
+        rgb.record_stream(st)
+        prim.record_stream(st)
+        pb.check(pb.lib.pt_render(scene.handle, C.byref(rd), rgb.data_ptr(), prim.data_ptr(), pb.MEM_DEVICE,
+                                  st.cuda_stream))
+        outs.append((rgb, prim, st))
+    for st in streams:
+        assert scene.status(st.cuda_stream) == pb.PT_OK
+    for (w, h, spp, seed, flags), (rgb, prim, st) in zip(frames, outs):
+        exp_rgb, exp_prim = pb.render(scene, w, h, spp, 4, W.SMALL_CAMERA, seed, flags)
+        assert_bit_equal(rgb.cpu().numpy().reshape(h, w, 3), exp_rgb, f"film {w}x{h}")
+        assert_bit_equal(prim.cpu().numpy().view(np.uint32).reshape(h, w), exp_prim, f"prim {w}x{h}")
 
 
 def test_runner_interface(cuda_device):

@@ -32,24 +32,33 @@ def test_noalloc_render_matches_pt_render_on_consecutive_calls(cuda_device):
     import torch
     meshes, env = W.small_scene(level=3)
     scene = pb.Scene(meshes, env)
-    # two calls in a row with different frames: the second reuses (and must clear) the scratch
-    for (w, h, spp, seed, flags) in ((64, 48, 3, 1, pb.RENDER_NEE), (40, 30, 2, 5, pb.RENDER_NEE | pb.RENDER_JITTER)):
-        desc = pb.render_desc(w, h, spp, 4, W.SMALL_CAMERA, seed, flags)
+    # calls in a row with different frames: each reuses (and must clear) the scratch; the last two
+    # have more paths than one wave of the fixed array (262,144), so their waves loop over it
+    frames = ((64, 48, 3, 1, pb.RENDER_NEE, 0), (40, 30, 2, 5, pb.RENDER_NEE | pb.RENDER_JITTER, 0),
+              (256, 256, 8, 2, pb.RENDER_NEE, 0), (97, 61, 5, 3, pb.RENDER_NEE | pb.RENDER_FUSED, 7001))
+    for (w, h, spp, seed, flags, wave) in frames:
+        desc = pb.render_desc(w, h, spp, 4, W.SMALL_CAMERA, seed, flags, wave)
         got_rgb, got_prim = render_noalloc(scene, desc, torch, cuda_device)
         exp_rgb, exp_prim = pb.render(scene, w, h, spp, 4, W.SMALL_CAMERA, seed, flags)
-        assert got_rgb.tobytes() == exp_rgb.tobytes()
-        assert got_prim.tobytes() == exp_prim.tobytes()
+        assert got_rgb.tobytes() == exp_rgb.tobytes(), (w, h, spp)
+        assert got_prim.tobytes() == exp_prim.tobytes(), (w, h, spp)
         assert exp_rgb.mean() > 0
+    assert scene.status() == pb.PT_OK
 
 
 def test_noalloc_rejects_frames_above_its_limit(cuda_device):
     import torch
     meshes, env = W.small_scene(level=2)
     scene = pb.Scene(meshes, env)
-    desc = pb.render_desc(1024, 1024, 1, 2, W.SMALL_CAMERA)
-    assert pb.lib.pt_render_noalloc(scene.handle, C.byref(desc), None, None, None) == pb.PT_EINVAL
-    out = torch.zeros(600 * 600 * 3, dtype=torch.float32, device=cuda_device)  # a valid buffer, never written
-    desc = pb.render_desc(600, 600, 1, 2, W.SMALL_CAMERA)
-    rc = pb.lib.pt_render_noalloc(scene.handle, C.byref(desc), out.data_ptr(), None, None)
-    assert rc == pb.PT_EINVAL and "limit" in pb.last_error()
+    for (w, h) in ((1024, 1024), (600, 600), (512, 513)):
+        out = torch.zeros(w * h * 3, dtype=torch.float32, device=cuda_device)  # a valid buffer, never written
+        desc = pb.render_desc(w, h, 1, 2, W.SMALL_CAMERA)
+        rc = pb.lib.pt_render_noalloc(scene.handle, C.byref(desc), out.data_ptr(), None, None)
+        assert rc == pb.PT_EINVAL and "limit" in pb.last_error(), (w, h)
+        assert float(out.abs().sum()) == 0.0
+    # the other pipelines are refused, not silently replaced by the fused one
+    out = torch.zeros(16 * 16 * 3, dtype=torch.float32, device=cuda_device)
+    for fl in (pb.RENDER_PERSISTENT, pb.RENDER_WAVEFRONT):
+        desc = pb.render_desc(16, 16, 1, 2, W.SMALL_CAMERA, 1, fl)
+        assert pb.lib.pt_render_noalloc(scene.handle, C.byref(desc), out.data_ptr(), None, None) == pb.PT_EINVAL
     assert float(out.abs().sum()) == 0.0
