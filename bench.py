@@ -105,27 +105,37 @@ def build_scenes(pb, specs, threads=16):
 
 
 def bench_batched(pb, torch, n_scenes=256):
-    """256 uneven scenes: one autotuned batched launch vs one plain pt_render launch per scene."""
+    """256 uneven scenes: one autotuned batched launch vs one plain pt_render launch per scene, the
+    plain launch both with pt_render's default pipeline (the persistent path kernel, the fastest
+    single-frame launch) and with the one-thread-per-path fused kernel."""
     import ctypes as C
     from polytope_b200 import workloads as W
     work = W.batched_workload(n_scenes)
     scenes = build_scenes(pb, [(w[0], w[1]) for w in work])
     jobs = [(sc, pb.render_desc(d["width"], d["height"], d["spp"], d["max_depth"], d["camera"], d["seed"], pb.RENDER_NEE))
             for sc, (_, _, d) in zip(scenes, work)]
+    fused = [(sc, pb.render_desc(d["width"], d["height"], d["spp"], d["max_depth"], d["camera"], d["seed"],
+                                 pb.RENDER_NEE | pb.RENDER_FUSED)) for sc, (_, _, d) in zip(scenes, work)]
     outs = [torch.empty(rd.width * rd.height * 3, dtype=torch.float32, device="cuda") for _, rd in jobs]
-
-    def plain():
-        for (sc, rd), o in zip(jobs, outs):
-            pb.check(pb.lib.pt_render(sc.handle, C.byref(rd), o.data_ptr(), None, pb.MEM_DEVICE, None))
-    for (sc, rd), o in zip(jobs[:8], outs):
-        pb.check(pb.lib.pt_render(sc.handle, C.byref(rd), o.data_ptr(), None, pb.MEM_DEVICE, None))
-    torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    plain()
-    e1.record()
-    e1.synchronize()
-    plain_ms = e0.elapsed_time(e1)
+
+    def plain(js):
+        # pt_render with device films only queues its work, so the events bracket the GPU time of
+        # 256 back-to-back frames on the stream
+        for (sc, rd), o in zip(js[:8], outs):
+            pb.check(pb.lib.pt_render(sc.handle, C.byref(rd), o.data_ptr(), None, pb.MEM_DEVICE, None))
+        torch.cuda.synchronize()
+        e0.record()
+        for (sc, rd), o in zip(js, outs):
+            pb.check(pb.lib.pt_render(sc.handle, C.byref(rd), o.data_ptr(), None, pb.MEM_DEVICE, None))
+        e1.record()
+        e1.synchronize()
+        for sc, _ in js[:1]:
+            assert sc.status() == pb.PT_OK
+        return e0.elapsed_time(e1)
+
+    plain_ms = plain(jobs)
+    fused_ms = plain(fused)
     best, _, trials = pb.autotune(jobs[::8])
     b = pb.Batch(jobs, best)
     b.run()
@@ -140,9 +150,12 @@ def bench_batched(pb, torch, n_scenes=256):
             "tris": int(sum(sum(len(m.faces) for m in w[0]) for w in work)),
             "paths": int(sum(rd.width * rd.height * rd.spp for _, rd in jobs)), "rays": int(rays),
             "plain_ms": round(plain_ms, 2), "plain_mrays_s": round(rays / plain_ms / 1e3, 1),
+            "plain_fused_ms": round(fused_ms, 2), "plain_fused_mrays_s": round(rays / fused_ms / 1e3, 1),
             "batched_ms": round(batch_ms, 2), "batched_mrays_s": round(rays / batch_ms / 1e3, 1),
-            "speedup": round(plain_ms / batch_ms, 3), "tuning": best.as_dict(), "autotune_trials": len(trials),
-            "timing": "CUDA events around 256 sequential pt_render calls (device films) and around one batch graph replay"}
+            "speedup": round(plain_ms / batch_ms, 3), "speedup_vs_fused_plain": round(fused_ms / batch_ms, 3),
+            "tuning": best.as_dict(), "autotune_trials": len(trials),
+            "timing": "CUDA events around 256 sequential pt_render calls (device films; default pipeline = persistent "
+                      "path kernel, and PT_RENDER_FUSED) and around one batch graph replay"}
 
 
 def bench_render(pb, torch, cpu=True, cpu_rows=16, threads=None):
@@ -173,10 +186,16 @@ def bench_render(pb, torch, cpu=True, cpu_rows=16, threads=None):
             ts.append(e0.elapsed_time(e1))
         return statistics.median(ts)
 
+    rd_fused = pb.render_desc(d["width"], d["height"], d["spp"], d["max_depth"], d["camera"], d["seed"],
+                              pb.RENDER_NEE | pb.RENDER_FUSED)
+    fused_ms = timed(lambda: pb.check(pb.lib.pt_render(scene.handle, C.byref(rd_fused), out.data_ptr(), prim.data_ptr(),
+                                                       pb.MEM_DEVICE, None)))
+    fused_film = out.view(rd.height, rd.width, 3).cpu().numpy()
     plain_ms = timed(lambda: pb.check(pb.lib.pt_render(scene.handle, C.byref(rd), out.data_ptr(), prim.data_ptr(),
                                                        pb.MEM_DEVICE, None)))
     film = out.view(rd.height, rd.width, 3).cpu().numpy()
     prim_ids = prim.view(rd.height, rd.width).cpu().numpy().view(np.uint32)
+    assert scene.status() == pb.PT_OK
     best, _, trials = pb.autotune([(scene, rd)])
     b = pb.Batch([(scene, rd)], best)
     tuned_ms = timed(b.run)
@@ -185,7 +204,11 @@ def bench_render(pb, torch, cpu=True, cpu_rows=16, threads=None):
     b.close()
     res = {"workload": "instanced displaced spheres (5 x 1,310,720 + 2 tris), 1920x1080, 64 spp, depth 8, NEE",
            "samples": samples, "rays": int(rays),
-           "plain": {"ms": round(plain_ms, 2), "msamples_s": round(samples / plain_ms / 1e3, 1), "mrays_s": round(rays / plain_ms / 1e3, 1)},
+           "plain": {"ms": round(plain_ms, 2), "msamples_s": round(samples / plain_ms / 1e3, 1), "mrays_s": round(rays / plain_ms / 1e3, 1),
+                     "pipeline": "pt_render default (persistent path kernel)"},
+           "plain_fused": {"ms": round(fused_ms, 2), "msamples_s": round(samples / fused_ms / 1e3, 1),
+                           "mrays_s": round(rays / fused_ms / 1e3, 1), "pipeline": "PT_RENDER_FUSED",
+                           "film_equals_plain": bool(np.array_equal(fused_film.view(np.uint32), film.view(np.uint32)))},
            "autotuned": {"ms": round(tuned_ms, 2), "msamples_s": round(samples / tuned_ms / 1e3, 1),
                          "mrays_s": round(rays / tuned_ms / 1e3, 1), "tuning": best.as_dict(), "trials": len(trials)},
            "autotuned_equals_plain": bool(np.array_equal(tuned_film.view(np.uint32), film.view(np.uint32))
@@ -280,8 +303,19 @@ def run_served(pb, srv, scenes, reqs, arrivals, films=None):
     return lats, span, srv.stats()["rays_traced"] - rays0
 
 
+def with_flags(pb, reqs, extra):
+    """The same requests with extra render flags (a pipeline choice for the plain arm)."""
+    out = []
+    for si, rd in reqs:
+        r2 = pb.RenderDesc.from_buffer_copy(rd)
+        r2.flags = rd.flags | extra
+        out.append((si, r2))
+    return out
+
+
 def run_plain(pb, scenes, reqs, arrivals, films=None):
-    """One pt_render per request in arrival order (host film out); returns (latencies ms, makespan s)."""
+    """One pt_render per request in arrival order (host film out, pt_render's default pipeline
+    unless the requests carry another); returns (latencies ms, makespan s)."""
     films = films or film_buffers(reqs)
     done = np.zeros(len(reqs))
     t0 = time.perf_counter()
@@ -320,11 +354,15 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
         return {"mrays_s": round(rays / span / 1e6, 1), "p50_ms": pct(lat, 50), "p95_ms": pct(lat, 95),
                 "p99_ms": pct(lat, 99), "makespan_s": round(span, 3)}
 
+    fused_reqs = with_flags(pb, reqs, pb.RENDER_FUSED)
+    run_plain(pb, scenes, fused_reqs, np.zeros(len(reqs)), films)
     for rate in rates:
         # both arms are host-clocked, so each rate runs `repeats` times, arms alternating, and the
-        # run with the median makespan of each arm is reported (all runs listed beside it)
+        # run with the median makespan of each arm is reported (all runs listed beside it); at the
+        # highest rate the plain arm also runs with the one-thread-per-path fused kernel
         arrivals = unit / rate
-        served, plain = [], []
+        top = rate == max(rates)
+        served, plain, plain_fused = [], [], []
         for _ in range(repeats):
             s0 = srv.stats()
             lat_s, span_s, rays = run_served(pb, srv, scenes, reqs, arrivals, films)
@@ -332,16 +370,37 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
             served.append(summary(lat_s, span_s, rays))
             served[-1]["gpu_busy_ms"] = round(s1["busy_ms"] - s0["busy_ms"], 1)
             served[-1]["waves"] = int(s1["waves"] - s0["waves"])
+            served[-1]["blocked_admission_ms"] = round(s1["blocked_ms"] - s0["blocked_ms"], 1)
             lat_p, span_p = run_plain(pb, scenes, reqs, arrivals, films)
             plain.append(summary(lat_p, span_p, rays))
+            if top:
+                lat_f, span_f = run_plain(pb, scenes, fused_reqs, arrivals, films)
+                plain_fused.append(summary(lat_f, span_f, rays))
         med = lambda runs: sorted(runs, key=lambda r: r["makespan_s"])[len(runs) // 2]
         out["rays"] = int(rays)
-        out["rates"].append({
-            "rate_per_s": rate,
-            "served": med(served), "plain_per_request": med(plain),
-            "runs": {"served": [(r["mrays_s"], r["p99_ms"], r["gpu_busy_ms"]) for r in served],
-                     "plain_per_request": [(r["mrays_s"], r["p99_ms"]) for r in plain]}})
+        entry = {"rate_per_s": rate, "served": med(served), "plain_per_request": med(plain),
+                 "runs": {"served": [(r["mrays_s"], r["p99_ms"], r["gpu_busy_ms"]) for r in served],
+                          "plain_per_request": [(r["mrays_s"], r["p99_ms"]) for r in plain]}}
+        entry["served_over_plain"] = round(entry["served"]["mrays_s"] / entry["plain_per_request"]["mrays_s"], 3)
+        if top:
+            entry["plain_per_request_fused"] = med(plain_fused)
+            entry["runs"]["plain_per_request_fused"] = [(r["mrays_s"], r["p99_ms"]) for r in plain_fused]
+            entry["served_over_plain_fused"] = round(entry["served"]["mrays_s"] / entry["plain_per_request_fused"]["mrays_s"], 3)
+        out["rates"].append(entry)
     srv.close()
+    # admission by device memory: the same requests at the highest rate under a request-memory
+    # budget of 256 MiB (about nine 1024x1024 requests), so admissions wait for memory to free up
+    budget = 256 << 20
+    bsrv = pb.Server(max_inflight=64, memory_budget=budget, wave_pixels=1 << 25, tuning=serve_tuning(pb),
+                     host_budget=2 << 30)
+    run_served(pb, bsrv, scenes, reqs, np.zeros(len(reqs)), films)
+    s0 = bsrv.stats()
+    lat_b, span_b, rays_b = run_served(pb, bsrv, scenes, reqs, unit / max(rates), films)
+    s1 = bsrv.stats()
+    out["memory_budgeted"] = dict(summary(lat_b, span_b, rays_b), rate_per_s=max(rates), memory_budget_bytes=budget,
+                                  blocked_admission_ms=round(s1["blocked_ms"] - s0["blocked_ms"], 1),
+                                  gpu_busy_ms=round(s1["busy_ms"] - s0["busy_ms"], 1))
+    bsrv.close()
     return out
 
 

@@ -46,6 +46,7 @@ extern "C" {
 #define PT_ETIMEOUT (-3)   /* a bounded device wait ran out                                */
 #define PT_ECUDA    (-4)   /* CUDA runtime error or no device                              */
 #define PT_ESTACK   (-5)   /* traversal stack capacity exceeded (tree deeper than capacity) */
+#define PT_ECANCELED (-6)  /* the served request was cancelled (pt_server_cancel)           */
 
 /* ---- geometry ---------------------------------------------------------------------------- */
 
@@ -223,6 +224,15 @@ typedef struct pt_render_desc {
  *     which pt_scene_status reports. */
 int pt_render(pt_scene *scene, const pt_render_desc *desc, float *rgb_out,
               uint32_t *primary_prim_out, uint32_t mem_flags, void *stream);
+
+/* The render call followed by the reference's PNG output step on the device: the frame of
+ * pt_render, quantised as PNGFilm::Output stores it (src/cpu/films/PNGFilm.cpp:20-45; see
+ * pt_film_to_rgba8), so only width*height*4 bytes leave the device instead of the 12-byte float
+ * film.  rgba_out: width*height*4 bytes; primary_prim_out as in pt_render (optional).  Pointers
+ * follow mem_flags with pt_render's semantics (host: returns when the bytes are there and reports
+ * its own guard failures; PT_MEM_DEVICE: queued on `stream`, guard failures in pt_scene_status). */
+int pt_render_rgba8(pt_scene *scene, const pt_render_desc *desc, uint8_t *rgba_out,
+                    uint32_t *primary_prim_out, uint32_t mem_flags, void *stream);
 
 /* Waits for `stream`, then reports (PT_ESTACK) and clears the scene's device error flag: set when
  * a kernel of an asynchronous call on this scene (pt_render or pt_trace with PT_MEM_DEVICE,
@@ -445,6 +455,7 @@ typedef struct pt_server_stats {
     double   plan_ms;                 /* scheduler time admitting, planning and enqueueing waves  */
     double   retire_wait_ms;          /* scheduler time waiting for waves and their film copies   */
     uint64_t waves_launched;          /* waves enqueued (waves counts retired ones)               */
+    uint64_t cancelled;               /* requests ended by pt_server_cancel                       */
 } pt_server_stats;
 
 typedef struct pt_server pt_server;
@@ -453,8 +464,8 @@ typedef struct pt_server pt_server;
  * runs waves that take work from the admitted requests by the configured policy, so requests
  * arriving while others run join the next wave.  Two waves stay queued on the GPU while the host
  * plans the next one and copies finished films out.  Request states: 0 queued, 1 admitted,
- * 2 done, < 0 error.  A request's film is identical to pt_render's whether it ran alone or in
- * any mix.  No counterpart in the reference, which renders one frame per process. */
+ * 2 done, 3 cancelled, < 0 error.  A request's film is identical to pt_render's whether it ran
+ * alone or in any mix.  No counterpart in the reference, which renders one frame per process. */
 int pt_server_create(const pt_server_config *cfg, pt_server **out);
 int pt_server_submit(pt_server *server, pt_scene *scene, const pt_render_desc *desc, uint64_t *ticket);
 /* latency_ms: submit to completion (-1 until done). */
@@ -467,8 +478,16 @@ typedef struct pt_request_timing {
     double admitted_ms, first_wave_ms, last_wave_ms, done_ms;
 } pt_request_timing;
 int pt_server_timing(pt_server *server, uint64_t ticket, pt_request_timing *timing);
-/* Copies a finished request's film (width*height*3 floats) and primary ids, then forgets it. */
+/* Copies a finished request's film (width*height*3 floats) and primary ids, then forgets it.  A
+ * failed or cancelled request is forgotten too, and its status (PT_ECANCELED for a cancelled one)
+ * is returned. */
 int pt_server_fetch(pt_server *server, uint64_t ticket, float *rgb_out, uint32_t *primary_out);
+/* Cancels a request.  A queued one ends at once (state 3); an admitted one gets no work in later
+ * waves, and ends (state 3, its device memory and host arena space released) once the waves
+ * already queued with its work have retired -- at most two, the scheduler's queue depth.  Waiting
+ * for it with pt_server_wait then returns state 3.  PT_EINVAL for an unknown ticket or a request
+ * that has already finished (done, failed or cancelled). */
+int pt_server_cancel(pt_server *server, uint64_t ticket);
 int pt_server_get_stats(pt_server *server, pt_server_stats *stats);
 int pt_server_destroy(pt_server *server);
 

@@ -26,7 +26,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libpolytope_b200.so")
 
-PT_OK, PT_EINVAL, PT_ENOMEM, PT_ETIMEOUT, PT_ECUDA, PT_ESTACK = 0, -1, -2, -3, -4, -5
+PT_OK, PT_EINVAL, PT_ENOMEM, PT_ETIMEOUT, PT_ECUDA, PT_ESTACK, PT_ECANCELED = 0, -1, -2, -3, -4, -5, -6
+REQ_QUEUED, REQ_ADMITTED, REQ_DONE, REQ_CANCELLED = 0, 1, 2, 3
 PRIM_NONE = 0xFFFFFFFF
 MAT_LAMBERT, MAT_MIRROR = 1, 2
 RAY_ANY_HIT = 1
@@ -147,7 +148,7 @@ class ServerStats(C.Structure):
     _fields_ = [("waves", C.c_uint64), ("completed", C.c_uint64), ("rays_traced", C.c_uint64), ("busy_ms", C.c_double),
                 ("pending", C.c_uint64), ("active", C.c_uint64), ("device_bytes_in_use", C.c_uint64),
                 ("blocked_ms", C.c_double), ("host_bytes_in_use", C.c_uint64), ("plan_ms", C.c_double),
-                ("retire_wait_ms", C.c_double), ("waves_launched", C.c_uint64)]
+                ("retire_wait_ms", C.c_double), ("waves_launched", C.c_uint64), ("cancelled", C.c_uint64)]
 
 
 def _load() -> C.CDLL:
@@ -171,6 +172,7 @@ def _load() -> C.CDLL:
         "pt_trace_autotune": (i, [_vp, _vp, u64, _vp, C.POINTER(TraceTuning), C.POINTER(C.c_float)]),
         "pt_render_noalloc": (i, [_vp, C.POINTER(RenderDesc), _vp, _vp, _vp]),
         "pt_scene_status": (i, [_vp, _vp]),
+        "pt_render_rgba8": (i, [_vp, C.POINTER(RenderDesc), _vp, _vp, u32, _vp]),
         "pt_film_to_rgba8": (i, [_vp, u32, u32, _vp, u32, _vp]),
         "pt_load_ply": (i, [C.c_char_p, C.POINTER(MeshData)]),
         "pt_load_obj": (i, [C.c_char_p, C.POINTER(MeshData)]),
@@ -201,6 +203,7 @@ def _load() -> C.CDLL:
         "pt_server_fetch": (i, [_vp, u64, _vp, _vp]),
         "pt_server_get_stats": (i, [_vp, C.POINTER(ServerStats)]),
         "pt_server_destroy": (i, [_vp]),
+        "pt_server_cancel": (i, [_vp, u64]),
         "pt_gen_icosphere": (i, [u32, C.c_float, C.c_float, u64, _fp, _fp, _fp, _up, _up, _up, _up, _up]),
         "pt_gen_rays": (i, [u64, C.c_float, u64, _vp]),
         "pt_host_f64_diff_emulated": (C.c_float, [C.c_float] * 4),
@@ -424,6 +427,17 @@ def render(scene: Scene, width: int, height: int, spp: int, max_depth: int, came
     prim = np.zeros((height, width), np.uint32)
     check(lib.pt_render(scene.handle, C.byref(rd), rgb.ctypes.data, prim.ctypes.data, 0, None))
     return rgb, prim
+
+
+def render_rgba8(scene: Scene, width: int, height: int, spp: int, max_depth: int, camera: dict, seed: int = 1,
+                 flags: int = 0, wave_paths: int = 0):
+    """One frame as the reference's PNG output stores it, quantised on the device
+    (pt_render_rgba8): returns (RGBA8 (H, W, 4) uint8, primary prim ids (H, W) uint32)."""
+    rd = render_desc(width, height, spp, max_depth, camera, seed, flags, wave_paths)
+    rgba = np.zeros((height, width, 4), np.uint8)
+    prim = np.zeros((height, width), np.uint32)
+    check(lib.pt_render_rgba8(scene.handle, C.byref(rd), rgba.ctypes.data, prim.ctypes.data, 0, None))
+    return rgba, prim
 
 
 def load_ply(path: str, **mesh_kwargs) -> Mesh:
@@ -711,6 +725,11 @@ class Server:
         prim = np.zeros((rd.height, rd.width), np.uint32)
         check(lib.pt_server_fetch(self.handle, ticket, rgb.ctypes.data, prim.ctypes.data))
         return rgb, prim
+
+    def cancel(self, ticket: int) -> None:
+        """pt_server_cancel: a queued request ends at once; an admitted one after the waves already
+        queued with its work (its state then reads REQ_CANCELLED)."""
+        check(lib.pt_server_cancel(self.handle, ticket))
 
     def stats(self) -> dict:
         s = ServerStats()

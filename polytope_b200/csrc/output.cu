@@ -7,6 +7,7 @@
 #include <string>
 
 #include "pt_internal.h"
+#include "render.h"
 
 namespace pt {
 
@@ -22,6 +23,12 @@ __global__ void __launch_bounds__(256) rgba8_kernel(const float* __restrict__ rg
     if (i >= npix) return;
     const float r = rgb[3 * (size_t)i], g = rgb[3 * (size_t)i + 1], b = rgb[3 * (size_t)i + 2];
     out[i] = make_uchar4(quantize_channel(r), quantize_channel(g), quantize_channel(b), 255);
+}
+
+cudaError_t launch_film_to_rgba8(const float* rgb, uint32_t npix, uint8_t* rgba, cudaStream_t s) {
+    if (npix == 0) return cudaSuccess;
+    rgba8_kernel<<<(npix + 255) / 256, 256, 0, s>>>(rgb, npix, (uchar4*)rgba);
+    return cudaGetLastError();
 }
 
 }  // namespace pt
@@ -41,8 +48,7 @@ extern "C" int pt_film_to_rgba8(const float* rgb_dev, uint32_t width, uint32_t h
         cudaGetLastError();
         return fail(PT_ENOMEM, "device memory for the RGBA8 film");
     }
-    rgba8_kernel<<<(unsigned)((npix + 255) / 256), 256, 0, st>>>(rgb_dev, (uint32_t)npix, (uchar4*)out);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = launch_film_to_rgba8(rgb_dev, (uint32_t)npix, (uint8_t*)out, st);
     if (!dev_out) {
         if (e == cudaSuccess) e = cudaMemcpyAsync(rgba_out, out, 4 * npix, cudaMemcpyDeviceToHost, st);
         cudaFreeAsync(out, st);

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "batch.h"
 #include "launch.h"
@@ -63,6 +64,34 @@ __global__ void finish_kernel(const float* __restrict__ film, uint32_t npix, uin
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= 3 * npix) return;
     rgb[i] = fmul(film[i], frcp((float)spp));  // accum *= 1.0f / numSamples (BoxFilter.cpp:65-67)
+}
+
+// ---- small host -> device uploads without a stream sync --------------------------------------------
+//
+// cudaMemcpyAsync from pageable host memory waits for the work already queued on the stream before
+// it copies, so a frame's parameter tables copied that way would hold the caller until the previous
+// frame on the stream has finished.  Kernel parameters are captured at launch instead: the tables
+// travel as by-value blocks of a copy kernel, queued behind the earlier work like any launch.
+struct UploadBlock {
+    uint32_t words[960];  // 3840 bytes per launch, inside the 4 KB kernel-parameter space
+};
+
+__global__ void __launch_bounds__(256) upload_kernel(const UploadBlock blk, uint32_t nwords, uint32_t* __restrict__ dst) {
+    for (uint32_t i = threadIdx.x; i < nwords; i += blockDim.x) dst[i] = blk.words[i];
+}
+
+cudaError_t upload_async(void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if ((bytes & 3u) || ((uintptr_t)dst & 3u)) return cudaErrorInvalidValue;
+    const size_t per = sizeof(UploadBlock::words);
+    for (size_t off = 0; off < bytes; off += per) {
+        const size_t n = bytes - off < per ? bytes - off : per;
+        UploadBlock blk;
+        std::memcpy(blk.words, (const char*)src + off, n);
+        upload_kernel<<<1, 256, 0, s>>>(blk, (uint32_t)(n / 4), (uint32_t*)((char*)dst + off));
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 // ---- launchers ----------------------------------------------------------------------------------
@@ -179,42 +208,30 @@ int check_render_desc(const pt_scene* s, const pt_render_desc* desc) {
 }
 }  // namespace pt
 
-extern "C" int pt_render(pt_scene* s, const pt_render_desc* desc, float* rgb_out, uint32_t* primary_out,
-                         uint32_t mem_flags, void* stream) {
-    int rc = check_render_desc(s, desc);
-    if (rc) return rc;
-    if (!rgb_out) return fail(PT_EINVAL, "rgb_out is NULL");
+namespace {
+// Queues one frame on `st`: every wave, the film sums and the finished film into rgb_d (device),
+// sample 0's primary ids into prim_d (device, optional).  Guard failures raise `err`.  The
+// temporaries come from the render pool and go back to it in stream order, so nothing here waits
+// for the device.
+int enqueue_frame(pt_scene* s, const pt_render_desc* desc, float* rgb_d, uint32_t* prim_d, int* err, cudaStream_t st) {
     const uint64_t npix64 = (uint64_t)desc->width * desc->height;
     const uint32_t npix = (uint32_t)npix64;
-    int prev = -1;
-    cudaGetDevice(&prev);
-    if (prev != s->device) cudaSetDevice(s->device);
-    struct Restore { int d; ~Restore() { if (d >= 0) cudaSetDevice(d); } } restore{prev != s->device ? prev : -1};
-
-    const bool dev_out = (mem_flags & PT_MEM_DEVICE) != 0;
     RenderParams p = render_params(s, desc);
+    p.err = err;
     // Pipelines: the persistent path kernel unless PT_RENDER_FUSED or PT_RENDER_WAVEFRONT is given
     // (the wave engine runs both the queue-based kernels and the persistent path kernel).
     const bool fused = (desc->flags & PT_RENDER_FUSED) != 0;
     const bool persistent = !fused && (desc->flags & PT_RENDER_WAVEFRONT) == 0;
     const bool wavefront = !fused;
-    cudaStream_t st = (cudaStream_t)stream;
     const uint64_t total = npix64 * desc->spp;
     // Default wave: 4 M paths for the fused and queue-based kernels (the queues cost ~140 B per
     // path), 32 M for the persistent path kernel (12 B per path; longer waves shorten its tail).
     uint64_t wave = desc->wave_paths ? desc->wave_paths : (persistent ? (1ull << 25) : (1ull << 22));
     if (wave > total) wave = total;
     cudaMemPool_t pool = render_pool(s->device);
-    DevBuf rad, film, rgb_dev, prim_dev, wsbuf, tables;
-    // the film sums, then (host-memory calls) this call's own error flag
-    const size_t film_bytes = (12 * (size_t)npix + 15) & ~(size_t)15;
-    if ((!wavefront && !rad.alloc(12 * (size_t)wave, pool, st)) || !film.alloc(film_bytes + 16, pool, st))
+    DevBuf rad, film, wsbuf, tables;
+    if ((!wavefront && !rad.alloc(12 * (size_t)wave, pool, st)) || !film.alloc(12 * (size_t)npix, pool, st))
         return fail(PT_ENOMEM, "device memory for the render buffers");
-    // A host-memory call waits for its frame and reports a guard failure of its own kernels; a
-    // device-memory call returns once the work is queued, and its kernels raise the scene's flag,
-    // which pt_scene_status reads.
-    int* call_err = (int*)((char*)film.p + film_bytes);
-    p.err = dev_out ? (int*)s->err_flag : call_err;
     WfState ws{};
     WfPlan plan;
     if (wavefront) {
@@ -223,27 +240,16 @@ extern "C" int pt_render(pt_scene* s, const pt_render_desc* desc, float* rgb_out
         wf_state_carve(wsbuf.p, (uint32_t)wave, ws, persistent);
         wf_plan_all(plan, {npix}, {desc->spp}, {desc->max_depth}, wave);
     }
-    float* rgb_d = rgb_out;
-    uint32_t* prim_d = primary_out;
-    if (!dev_out) {
-        if (!rgb_dev.alloc(12 * (size_t)npix, pool, st)) return fail(PT_ENOMEM, "device memory for the film");
-        rgb_d = (float*)rgb_dev.p;
-        if (primary_out) {
-            if (!prim_dev.alloc(4 * (size_t)npix, pool, st)) return fail(PT_ENOMEM, "device memory for the primary ids");
-            prim_d = (uint32_t*)prim_dev.p;
-        }
-    }
-    cudaError_t e = cudaMemsetAsync(film.p, 0, film_bytes + 16, st);
+    cudaError_t e = cudaMemsetAsync(film.p, 0, 12 * (size_t)npix, st);
     if (wavefront) {
-        // one item: device copies of its parameters and of the plan's tables, staged in one
-        // host block and copied with one call
+        // one item: device copies of its parameters and of the plan's tables
         const size_t pbytes = (sizeof(RenderParams) + 255) & ~(size_t)255;
         const size_t ibytes = (sizeof(WfItem) + 255) & ~(size_t)255;
         const size_t sbytes = ((sizeof(WfSegment) * plan.segments.size()) + 255) & ~(size_t)255;
         const size_t rbytes = ((sizeof(WfPixels) * plan.resolve.size()) + 255) & ~(size_t)255;
         const size_t fbytes = sizeof(WfPixels) * plan.finish.size();
-        const size_t tbytes = pbytes + ibytes + sbytes + rbytes + fbytes;
-        if (!tables.alloc(tbytes, pool, st)) return fail(PT_ENOMEM, "device memory for the wavefront tables");
+        if (!tables.alloc(((pbytes + ibytes + sbytes + rbytes + fbytes) + 3) & ~(size_t)3, pool, st))
+            return fail(PT_ENOMEM, "device memory for the wavefront tables");
         char* tb = (char*)tables.p;
         RenderParams* d_params = (RenderParams*)tb;
         WfItem* d_item = (WfItem*)(tb + pbytes);
@@ -251,11 +257,14 @@ extern "C" int pt_render(pt_scene* s, const pt_render_desc* desc, float* rgb_out
         WfPixels* d_res = (WfPixels*)(tb + pbytes + ibytes + sbytes);
         WfPixels* d_fin = (WfPixels*)(tb + pbytes + ibytes + sbytes + rbytes);
         const WfItem item{d_params, (float*)film.p, rgb_d, prim_d, npix, desc->spp};
-        if (e == cudaSuccess) e = cudaMemcpyAsync(d_params, &p, sizeof(p), cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(d_item, &item, sizeof(item), cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(d_segs, plan.segments.data(), sizeof(WfSegment) * plan.segments.size(), cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(d_res, plan.resolve.data(), sizeof(WfPixels) * plan.resolve.size(), cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(d_fin, plan.finish.data(), sizeof(WfPixels) * plan.finish.size(), cudaMemcpyHostToDevice, st);
+        // the tables in one host block, uploaded without waiting for the stream's earlier work
+        std::vector<char> host(((pbytes + ibytes + sbytes + rbytes + fbytes) + 3) & ~(size_t)3, 0);
+        std::memcpy(host.data(), &p, sizeof(p));
+        std::memcpy(host.data() + pbytes, &item, sizeof(item));
+        std::memcpy(host.data() + pbytes + ibytes, plan.segments.data(), sizeof(WfSegment) * plan.segments.size());
+        std::memcpy(host.data() + pbytes + ibytes + sbytes, plan.resolve.data(), sizeof(WfPixels) * plan.resolve.size());
+        std::memcpy(host.data() + pbytes + ibytes + sbytes + rbytes, plan.finish.data(), sizeof(WfPixels) * plan.finish.size());
+        if (e == cudaSuccess) e = upload_async(tb, host.data(), host.size(), st);
         WfTuning t;
         t.stack_cap = stack_cap_for(s->max_depth, 0);
         t.paths = persistent;
@@ -270,13 +279,84 @@ extern "C" int pt_render(pt_scene* s, const pt_render_desc* desc, float* rgb_out
         if (e == cudaSuccess) e = launch_finish_film((const float*)film.p, npix, desc->spp, rgb_d, st);
     }
     if (e != cudaSuccess) return fail(PT_ECUDA, std::string("render launch: ") + cudaGetErrorString(e));
-    // Device-memory output: the temporaries go back to the pool in stream order, so nothing here
-    // waits for the frame.
+    return PT_OK;
+}
+
+struct DeviceScope {  // makes the scene's device current for the call, restores the caller's
+    int prev = -1;
+    explicit DeviceScope(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev); else prev = -1;
+    }
+    ~DeviceScope() { if (prev >= 0) cudaSetDevice(prev); }
+};
+}  // namespace
+
+extern "C" int pt_render(pt_scene* s, const pt_render_desc* desc, float* rgb_out, uint32_t* primary_out,
+                         uint32_t mem_flags, void* stream) {
+    int rc = check_render_desc(s, desc);
+    if (rc) return rc;
+    if (!rgb_out) return fail(PT_EINVAL, "rgb_out is NULL");
+    DeviceScope scope(s->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    // Device-memory output: the frame is only queued, and a guard failure raises the scene's flag
+    // (pt_scene_status).
+    if (mem_flags & PT_MEM_DEVICE) return enqueue_frame(s, desc, rgb_out, primary_out, (int*)s->err_flag, st);
+    // Host-memory output: device film, primary ids and this call's own error flag, then copies out
+    // and a wait for the frame.
+    const size_t npix = (size_t)desc->width * desc->height;
+    cudaMemPool_t pool = render_pool(s->device);
+    DevBuf out;
+    const size_t rgb_bytes = 12 * npix, prim_bytes = primary_out ? 4 * npix : 0;
+    if (!out.alloc(rgb_bytes + prim_bytes + 16, pool, st)) return fail(PT_ENOMEM, "device memory for the film");
+    float* rgb_d = (float*)out.p;
+    uint32_t* prim_d = primary_out ? (uint32_t*)((char*)out.p + rgb_bytes) : nullptr;
+    int* call_err = (int*)((char*)out.p + ((rgb_bytes + prim_bytes + 15) & ~(size_t)15));
+    cudaError_t e = cudaMemsetAsync(call_err, 0, sizeof(int), st);
+    if (e != cudaSuccess) return fail(PT_ECUDA, std::string("render: ") + cudaGetErrorString(e));
+    rc = enqueue_frame(s, desc, rgb_d, prim_d, call_err, st);
+    if (rc) return rc;
+    int err = 0;
+    e = cudaMemcpyAsync(rgb_out, rgb_d, rgb_bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && primary_out) e = cudaMemcpyAsync(primary_out, prim_d, prim_bytes, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&err, call_err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail(PT_ECUDA, std::string("render: ") + cudaGetErrorString(e));
+    if (err) return fail(PT_ESTACK, "a path exceeded the traversal stack");
+    return PT_OK;
+}
+
+extern "C" int pt_render_rgba8(pt_scene* s, const pt_render_desc* desc, uint8_t* rgba_out, uint32_t* primary_out,
+                               uint32_t mem_flags, void* stream) {
+    int rc = check_render_desc(s, desc);
+    if (rc) return rc;
+    if (!rgba_out) return fail(PT_EINVAL, "rgba_out is NULL");
+    DeviceScope scope(s->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const bool dev_out = (mem_flags & PT_MEM_DEVICE) != 0;
+    const size_t npix = (size_t)desc->width * desc->height;
+    cudaMemPool_t pool = render_pool(s->device);
+    // the float film stays on the device; host-memory calls also stage the bytes, the primary ids
+    // and their own error flag there
+    const size_t rgb_bytes = 12 * npix, byte_bytes = dev_out ? 0 : 4 * npix;
+    const size_t prim_bytes = (!dev_out && primary_out) ? 4 * npix : 0;
+    DevBuf tmp;
+    if (!tmp.alloc(rgb_bytes + byte_bytes + prim_bytes + 16, pool, st)) return fail(PT_ENOMEM, "device memory for the film");
+    float* rgb_d = (float*)tmp.p;
+    uint8_t* bytes_d = dev_out ? rgba_out : (uint8_t*)tmp.p + rgb_bytes;
+    uint32_t* prim_d = dev_out ? primary_out : (primary_out ? (uint32_t*)((char*)tmp.p + rgb_bytes + byte_bytes) : nullptr);
+    int* call_err = dev_out ? (int*)s->err_flag
+                            : (int*)((char*)tmp.p + ((rgb_bytes + byte_bytes + prim_bytes + 15) & ~(size_t)15));
+    cudaError_t e = dev_out ? cudaSuccess : cudaMemsetAsync(call_err, 0, sizeof(int), st);
+    if (e != cudaSuccess) return fail(PT_ECUDA, std::string("render: ") + cudaGetErrorString(e));
+    rc = enqueue_frame(s, desc, rgb_d, prim_d, call_err, st);
+    if (rc) return rc;
+    e = launch_film_to_rgba8(rgb_d, (uint32_t)npix, bytes_d, st);
+    if (e != cudaSuccess) return fail(PT_ECUDA, std::string("film to RGBA8: ") + cudaGetErrorString(e));
     if (dev_out) return PT_OK;
     int err = 0;
-    e = cudaMemcpyAsync(rgb_out, rgb_d, 12 * (size_t)npix, cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess && primary_out)
-        e = cudaMemcpyAsync(primary_out, prim_d, 4 * (size_t)npix, cudaMemcpyDeviceToHost, st);
+    e = cudaMemcpyAsync(rgba_out, bytes_d, 4 * npix, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess && primary_out) e = cudaMemcpyAsync(primary_out, prim_d, prim_bytes, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&err, call_err, sizeof(int), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return fail(PT_ECUDA, std::string("render: ") + cudaGetErrorString(e));
@@ -286,10 +366,7 @@ extern "C" int pt_render(pt_scene* s, const pt_render_desc* desc, float* rgb_out
 
 extern "C" int pt_scene_status(pt_scene* s, void* stream) {
     if (!s) return fail(PT_EINVAL, "scene is NULL");
-    int prev = -1;
-    cudaGetDevice(&prev);
-    if (prev != s->device) cudaSetDevice(s->device);
-    struct Restore { int d; ~Restore() { if (d >= 0) cudaSetDevice(d); } } restore{prev != s->device ? prev : -1};
+    DeviceScope scope(s->device);
     cudaStream_t st = (cudaStream_t)stream;
     int err = 0;
     cudaError_t e = cudaMemcpyAsync(&err, s->err_flag, sizeof(int), cudaMemcpyDeviceToHost, st);

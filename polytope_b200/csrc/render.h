@@ -45,6 +45,8 @@ cudaError_t launch_path_wave(const RenderParams& p, uint64_t first, uint32_t cou
 cudaError_t launch_resolve_wave(uint64_t first, uint32_t count, uint32_t num_pixels, const float* radiance,
                                 float* film_sum, cudaStream_t s);
 cudaError_t launch_finish_film(const float* film_sum, uint32_t num_pixels, uint32_t spp, float* rgb, cudaStream_t s);
+// rgb (3 floats per pixel) -> RGBA8 as PNGFilm::Output stores it (output.cu).
+cudaError_t launch_film_to_rgba8(const float* rgb, uint32_t num_pixels, uint8_t* rgba, cudaStream_t s);
 
 }  // namespace pt
 

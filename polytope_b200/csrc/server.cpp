@@ -55,8 +55,10 @@ struct Request {
     void* dev = nullptr;          // RenderParams, rgb (3 floats/px), primary ids, film sums (wave pipelines)
     size_t host_off = ~(size_t)0; // finished film in the host arena: rgb then primary ids
     uint32_t param_slot = ~0u;    // pinned staging slot of its parameters while admitted
-    int state = 0;                // 0 queued, 1 admitted, 2 done, < 0 error
+    int state = 0;                // 0 queued, 1 admitted, 2 done, 3 cancelled, < 0 error
     bool launched = false, retired = false;
+    bool cancel = false;          // pt_server_cancel while admitted: no more waves, then dropped
+    uint32_t waves_queued = 0;    // queued waves that hold work of this request
     Clock::time_point submitted, admitted, first_wave, last_wave, done;
 };
 
@@ -161,7 +163,7 @@ struct pt_server {
     char* h_tables = nullptr;
     size_t table_bytes = 0;
     // statistics
-    uint64_t waves = 0, completed = 0, rays_traced = 0;
+    uint64_t waves = 0, completed = 0, rays_traced = 0, cancelled = 0;
     double busy_ms = 0.0, blocked_ms = 0.0, plan_ms = 0.0, retire_wait_ms = 0.0;
     uint64_t waves_launched = 0;
     size_t host_in_use = 0;
@@ -172,9 +174,10 @@ struct pt_server {
     cudaError_t enqueue(WaveInFlight& w, const std::vector<uint32_t>& take, const std::vector<uint64_t>& first);
     void retire(WaveInFlight& w);
     void release_device(Request* r);  // with mu held
+    void finish_cancel(Request* r);   // with mu held
     bool has_unplanned() const {
         for (const Request* r : active)
-            if (r->state == 1 && r->planned < r->total) return true;
+            if (r->state == 1 && !r->cancel && r->planned < r->total) return true;
         return false;
     }
 };
@@ -241,7 +244,7 @@ void pt_server::plan(WaveInFlight& w, std::vector<uint32_t>& take, std::vector<u
     }
     for (Request* r : active) {
         if (w.members.size() >= max_items || room == 0) break;
-        if (r->state != 1 || r->planned >= r->total) continue;
+        if (r->state != 1 || r->cancel || r->planned >= r->total) continue;
         const uint64_t t = std::min<uint64_t>(std::min<uint64_t>(share, r->total - r->planned), room);
         room -= t;
         if (!r->launched) {
@@ -249,6 +252,7 @@ void pt_server::plan(WaveInFlight& w, std::vector<uint32_t>& take, std::vector<u
             r->first_wave = Clock::now();
         }
         w.members.push_back(r);
+        ++r->waves_queued;
         take.push_back((uint32_t)t);
         first.push_back(r->planned);
         r->planned += t;
@@ -355,6 +359,34 @@ void pt_server::release_device(Request* r) {
     blocked = false;
 }
 
+// Ends a cancelled request (mu held): its device memory goes back to the pool and its host arena
+// space is freed; the ticket stays until fetched.  No queued wave holds its work any more, and
+// every film copy of a wave that finished it has been waited for, so the only device work that
+// can still touch its memory is the parameter upload and film clear of its admission, queued on
+// the wave stream: the memory is freed in that stream's order.
+void pt_server::finish_cancel(Request* r) {
+    r->state = 3;
+    r->cancel = false;
+    if (r->param_slot != ~0u) {
+        free_param_slots.push_back(r->param_slot);
+        r->param_slot = ~0u;
+    }
+    if (r->dev) {
+        cudaFreeAsync(r->dev, stream);
+        r->dev = nullptr;
+        mem_in_use -= r->bytes;
+    }
+    r->done = Clock::now();
+    active.erase(std::remove(active.begin(), active.end(), r), active.end());
+    if (r->host_off != ~(size_t)0) {
+        arena_alloc.release(r->host_off, host_bytes(r->npix));
+        host_in_use -= host_bytes(r->npix);
+        r->host_off = ~(size_t)0;
+    }
+    ++cancelled;
+    blocked = false;
+}
+
 // Waits for a wave and the copies of the films it finished; those requests are done.
 void pt_server::retire(WaveInFlight& w) {
     cudaError_t e = w.launch;
@@ -367,15 +399,19 @@ void pt_server::retire(WaveInFlight& w) {
         std::lock_guard<std::mutex> lock(mu);
         busy_ms += ms;
         ++waves;
+        for (Request* r : w.members) --r->waves_queued;
         if (e == cudaSuccess) {
             rays_traced = h_rays[w.slot];
             for (Request* r : w.finishing) {
                 r->retired = true;
                 r->last_wave = kernels_done;
-                if (r->state != 1) continue;
+                if (r->state != 1 || r->cancel) continue;
                 r->state = 2;
                 release_device(r);
             }
+            // cancelled requests whose last queued wave this was
+            for (Request* r : w.members)
+                if (r->state == 1 && r->cancel && r->waves_queued == 0) finish_cancel(r);
         } else {
             worker_error = std::string("serving wave: ") + cudaGetErrorString(e);
             for (Request* r : w.members) {
@@ -590,7 +626,8 @@ extern "C" int pt_server_wait(pt_server* s, uint64_t ticket, uint32_t timeout_ms
     auto it = s->all.find(ticket);
     if (it == s->all.end()) return fail(PT_EINVAL, "unknown ticket");
     Request* r = it->second.get();
-    const bool ok = s->done_cv.wait_for(lock, std::chrono::milliseconds(timeout_ms), [&] { return r->state == 2 || r->state < 0; });
+    const bool ok = s->done_cv.wait_for(lock, std::chrono::milliseconds(timeout_ms),
+                                        [&] { return r->state == 2 || r->state == 3 || r->state < 0; });
     *state = r->state;
     if (!ok) return fail(PT_ETIMEOUT, "request not finished within the timeout");
     return PT_OK;
@@ -604,7 +641,8 @@ extern "C" int pt_server_fetch(pt_server* s, uint64_t ticket, float* rgb_out, ui
         std::lock_guard<std::mutex> lock(s->mu);
         auto it = s->all.find(ticket);
         if (it == s->all.end()) return fail(PT_EINVAL, "unknown ticket");
-        if (it->second->state != 2 && it->second->state >= 0) return fail(PT_EINVAL, "request not finished");
+        if (it->second->state != 2 && it->second->state != 3 && it->second->state >= 0)
+            return fail(PT_EINVAL, "request not finished");
         r = std::move(it->second);  // the ticket is gone; its arena block stays taken until released below
         s->all.erase(it);
         err = s->worker_error;
@@ -623,15 +661,40 @@ extern "C" int pt_server_fetch(pt_server* s, uint64_t ticket, float* rgb_out, ui
             s->host_in_use -= host_bytes(r->npix);
             s->blocked = false;
         }
-        if (r->state < 0) {
-            const int st = r->state;
+        if (r->state < 0 || r->state == 3) {
+            const int st = r->state == 3 ? PT_ECANCELED : r->state;
             // a failed request may still be named by a queued wave: keep it alive until destroy
             s->failed.push_back(std::move(r));
             s->cv.notify_one();
-            return fail(st, "request failed: " + err);
+            return st == PT_ECANCELED ? fail(st, "request was cancelled") : fail(st, "request failed: " + err);
         }
     }
     s->cv.notify_one();  // admission may have waited for arena space
+    return PT_OK;
+}
+
+extern "C" int pt_server_cancel(pt_server* s, uint64_t ticket) {
+    if (!s) return fail(PT_EINVAL, "server is NULL");
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        auto it = s->all.find(ticket);
+        if (it == s->all.end()) return fail(PT_EINVAL, "unknown ticket");
+        Request* r = it->second.get();
+        if (r->state == 0) {  // still queued: nothing of it is on the device
+            s->pending.erase(std::remove(s->pending.begin(), s->pending.end(), r), s->pending.end());
+            r->state = 3;
+            ++s->cancelled;
+        } else if (r->state == 1) {
+            if (r->cancel) return PT_OK;  // already being cancelled
+            r->cancel = true;
+            if (r->waves_queued == 0) s->finish_cancel(r);  // no queued wave holds its work
+            // otherwise the scheduler ends it when its last queued wave retires
+        } else {
+            return fail(PT_EINVAL, "request already finished");
+        }
+    }
+    s->done_cv.notify_all();
+    s->cv.notify_one();  // admission may have waited for the memory it held
     return PT_OK;
 }
 
@@ -650,6 +713,7 @@ extern "C" int pt_server_get_stats(pt_server* s, pt_server_stats* st) {
     st->plan_ms = s->plan_ms;
     st->retire_wait_ms = s->retire_wait_ms;
     st->waves_launched = s->waves_launched;
+    st->cancelled = s->cancelled;
     return PT_OK;
 }
 

@@ -23,6 +23,8 @@
 
 #include "cpu/acceleration/bvh.h"
 #include "cpu/cameras/AbstractCamera.h"
+#include "cpu/films/AbstractFilm.h"
+#include "cpu/films/PNGFilm.h"
 #include "cpu/runners/AbstractRunner.h"
 #include "cpu/scenes/Scene.h"
 #include "cpu/scenes/skyboxes/ColorSkybox.h"
@@ -159,12 +161,37 @@ inline pt_render_desc describe_render(const poly::AbstractRunner &runner, uint64
    return rd;
 }
 
+// A PNG film whose bytes were quantised on the device (pt_render_rgba8): Output() writes them to
+// the same file PNGFilm would (PNGFilm::Output, src/cpu/films/PNGFilm.cpp:20-58: clamp at 255,
+// truncation, alpha 255, then the PNG) through pt_write_png.  The film takes no samples.
+class DevicePNGFilm : public poly::AbstractFilm {
+public:
+   const std::string Filename;
+   std::vector<uint8_t> rgba;           // width * height * 4, filled by GpuRunner::Run
+   int status = PT_OK;
+
+   DevicePNGFilm(const poly::Bounds bounds, std::string filename)
+      : AbstractFilm(bounds, nullptr), Filename(std::move(filename)) {}
+
+   void AddSample(const poly::Point2f &, const poly::Sample &) override {}
+   void Output() override {
+      if (rgba.size() != 4 * (size_t) Bounds.x * Bounds.y) {
+         status = PT_EINVAL;
+         Log.error("DevicePNGFilm::Output: no rendered frame");
+         return;
+      }
+      status = pt_write_png(Filename.c_str(), rgba.data(), (uint32_t) Bounds.x, (uint32_t) Bounds.y);
+      if (status != PT_OK) Log.error(std::string("pt_write_png: ") + pt_last_error());
+   }
+};
+
 // Stands in for TileRunner in the render call (main.cpp:187-220): thread 0 renders the whole
-// frame with one pt_render call, the other threads return at once, and Output() then writes the
-// film through the reference's own PNGFilm.  Each pixel's value enters the film as one sample at
-// the pixel centre; BoxFilter::Output divides by the number of samples it holds (one), so the PNG
-// gets the rendered values unchanged.  A failed call leaves `status` at the PT_E* code and the
-// reason in Log.error; the film then stays empty.
+// frame with one library call, the other threads return at once, and Output() then writes the
+// film.  With a DevicePNGFilm (use_device_png) the frame is quantised on the device and only its
+// bytes come back; Output() writes them.  With any other film each pixel's float value enters the
+// film as one sample at the pixel centre; BoxFilter::Output divides by the number of samples it
+// holds (one), so the PNG gets the rendered values unchanged.  A failed call leaves `status` at the
+// PT_E* code and the reason in Log.error; the film then stays empty.
 class GpuRunner : public poly::AbstractRunner {
 public:
    GpuRunner(std::unique_ptr<poly::AbstractSampler> sampler, poly::Scene *scene,
@@ -177,11 +204,29 @@ public:
    uint64_t seed = 1;                   // counter-RNG key
    uint32_t flags = PT_RENDER_NEE;      // PT_RENDER_*
    int status = PT_OK;
-   std::vector<float> rgb;              // the float film, width * height * 3
+   std::vector<float> rgb;              // the float film, width * height * 3 (float-film mode)
+
+   // Replaces the runner's PNGFilm with a DevicePNGFilm writing the same file.  Returns false (and
+   // keeps the film) when the film is not a PNGFilm.
+   bool use_device_png() {
+      const auto *png = dynamic_cast<const poly::PNGFilm *>(Film.get());
+      if (png == nullptr) return false;
+      Film.reset(new DevicePNGFilm(Film->Bounds, png->Filename));
+      return true;
+   }
 
    void Run(int threadId) override {
       if (threadId != 0) return;
       const pt_render_desc rd = describe_render(*this, seed, flags);
+      if (auto *dev = dynamic_cast<DevicePNGFilm *>(Film.get())) {
+         dev->rgba.assign(4 * (size_t) rd.width * rd.height, 0);
+         status = pt_render_rgba8(gpu, &rd, dev->rgba.data(), nullptr, 0, nullptr);
+         if (status != PT_OK) {
+            dev->rgba.clear();
+            Log.error(std::string("pt_render_rgba8: ") + pt_last_error());
+         }
+         return;
+      }
       rgb.assign(3 * (size_t) rd.width * rd.height, 0.f);
       status = pt_render(gpu, &rd, rgb.data(), nullptr, 0, nullptr);
       if (status != PT_OK) {

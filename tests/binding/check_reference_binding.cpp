@@ -11,11 +11,22 @@
 //      file: geometry, matrices, materials, radiances, environment, and the render description;
 //   3. without a CUDA device, make_gpu_scene returns nullptr with the library's message and
 //      GpuRunner::Run records the failure instead of ending the process.
+// With `--render DIR THREADS` (needs a device) it then runs the render call of main.cpp:187-220
+// with GpuRunner in place of TileRunner -- Spawn(i) for each thread, join, Output() -- twice, on
+// fresh parses of the file: once into the reference's own PNGFilm (float film through BoxFilter
+// and lodepng) and once with DevicePNGFilm (quantised on the device, written by pt_write_png).  It
+// leaves DIR/film.bin (the float film), DIR/float_film.png and DIR/device_film.png for the test.
 // Prints one summary line and exits 0 when every check holds, 1 otherwise.
+//
+// Built by oracle/Makefile as oracle/_ref/check_reference_binding where the reference tree is
+// present (it needs the reference's headers), and by tests/test_reference_binding_cpu.py.
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "common/parsers/pbrt_parser.h"
@@ -35,6 +46,41 @@ static bool same_bits(const void *a, const void *b, size_t bytes) {
    if (bytes == 0) return true;
    if (a == nullptr || b == nullptr) return false;
    return std::memcmp(a, b, bytes) == 0;
+}
+
+// The render call as main.cpp:187-220 makes it, on a fresh parse of `path`, with GpuRunner in
+// place of the parsed TileRunner; `device_png` swaps the PNGFilm for a DevicePNGFilm.  The PNG the
+// film writes is moved to `dest`.  Returns the runner's float film (empty in device-PNG mode).
+static std::vector<float> render_once(const std::string &path, pt_scene *gpu, int threads, bool device_png,
+                                      const std::string &dest) {
+   poly::pbrt_parser parser;
+   std::unique_ptr<poly::AbstractRunner> parsed = parser.parse_file(path);
+   const auto *png = dynamic_cast<const poly::PNGFilm *>(parsed->Film.get());
+   check(png != nullptr, "the parsed film is a PNGFilm");
+   if (png == nullptr) return {};
+   const std::string written = png->Filename;
+   poly_b200::GpuRunner runner(std::move(parsed->Sampler), parsed->Scene, std::move(parsed->Integrator),
+                               std::move(parsed->Film), parsed->NumSamples, parsed->Bounds, gpu);
+   if (device_png) check(runner.use_device_png(), "use_device_png");
+   std::vector<std::thread> pool;
+   for (int i = 0; i < threads; ++i) pool.emplace_back(runner.Spawn(i));
+   for (auto &t : pool) t.join();
+   check(runner.status == PT_OK, std::string("GpuRunner::Run: ") + pt_last_error());
+   runner.Output();
+   if (device_png) {
+      const auto *dev = dynamic_cast<const poly_b200::DevicePNGFilm *>(runner.Film.get());
+      check(dev != nullptr && dev->status == PT_OK, "DevicePNGFilm::Output");
+   }
+   check(std::rename(written.c_str(), dest.c_str()) == 0, "the film wrote " + written);
+   return runner.rgb;
+}
+
+static void render_call(const std::string &path, pt_scene *gpu, const std::string &dir, int threads) {
+   const std::vector<float> film = render_once(path, gpu, threads, false, dir + "/float_film.png");
+   std::ofstream out(dir + "/film.bin", std::ios::binary);
+   out.write(reinterpret_cast<const char *>(film.data()), (std::streamsize) (film.size() * sizeof(float)));
+   check(out.good() && !film.empty(), "film.bin");
+   render_once(path, gpu, threads, true, dir + "/device_film.png");
 }
 
 int main(int argc, char **argv) {
@@ -119,6 +165,10 @@ int main(int argc, char **argv) {
    if (gpu == nullptr) {
       g.Run(0);
       check(g.status != PT_OK, "GpuRunner::Run without a device scene");
+   }
+   if (argc >= 5 && std::string(argv[2]) == "--render") {
+      check(gpu != nullptr, "--render needs a device scene: " + why);
+      if (gpu != nullptr) render_call(path, gpu, argv[3], std::atoi(argv[4]));
    }
    std::printf("meshes %u faces %llu nodes %u device %s\n", nm, (unsigned long long) faces, nn,
                gpu ? "yes" : ("no (" + why + ")").c_str());

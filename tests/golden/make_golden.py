@@ -17,7 +17,8 @@ Two kinds of fixture:
    bvh::bound / compact / intersect_compact / Mesh::intersect, and the patched render loop) on
    the seeded synthetic workloads, at sizes the CPU oracle finishes in seconds.
 
-Usage:  make -C oracle && python tests/golden/make_golden.py
+Usage:  make -C oracle && python tests/golden/make_golden.py [batch_box_scene]
+        (with the argument only batch_box_scene.npz is written)
 """
 from __future__ import annotations
 
@@ -176,9 +177,47 @@ def scene_inputs_digest(meshes) -> str:
     return sha(*[a for m in meshes for a in (m.x, m.y, m.z, m.faces, m.object_to_world)])
 
 
+def box_edge_rays(mesh, n_corner: int, n_edge: int, seed: int) -> np.ndarray:
+    """Closest-hit rays from random origins toward exact box corners and edge midpoints of a
+    boxes mesh (batched workload), where Wald edge functions can come out exactly zero."""
+    rng = np.random.default_rng(seed)
+    v = np.stack([mesh.x, mesh.y, mesh.z], 1).astype(np.float32)
+    tgt = np.concatenate([v[rng.integers(0, len(v), n_corner)],
+                          (0.5 * (v[0::8][:n_edge] + v[1::8][:n_edge])).astype(np.float32)])
+    org = rng.uniform(-6, 6, (len(tgt), 3)).astype(np.float32)
+    rays = np.zeros(len(tgt), po.RAY_DTYPE)
+    rays["org"] = org
+    d = tgt - org
+    rays["dir"] = (d / np.linalg.norm(d, axis=1)[:, None]).astype(np.float32)
+    rays["tmax"] = np.inf
+    return rays
+
+
+BOX_SCENE_INDEX = 12  # scene 12 of the 256-scene batched workload: 1,570 faces (104 boxes), 64x64, 64 spp
+
+
+def make_box_scene_fixture():
+    """Scene 12 of the batched workload (seed 23) rendered by the reference's patched render loop at
+    its own resolution, spp and depth (64x64, 64 spp, depth 6, NEE), plus closest hits and per-ray
+    node/face test counts of rays aimed at its box corners and edges."""
+    meshes, env, d = W.batched_workload(256)[BOX_SCENE_INDEX]
+    ref = po.RefScene(meshes, env)
+    nodes, pairs = ref.tree()
+    rays = box_edge_rays(meshes[1], 2048, 1024, 61)
+    hits, nt, tt = ref.trace(rays, counts=True)
+    rgb, prim = ref.render(dict(d, flags=1))
+    np.savez_compressed(os.path.join(HERE, "batch_box_scene.npz"), inputs_sha=scene_inputs_digest(meshes),
+                        tree_sha=sha(nodes, pairs), num_nodes=len(nodes), rays=rays, hits=hits, node_tests=nt,
+                        tri_tests=tt, rgb=rgb, prim=prim, width=d["width"], height=d["height"], spp=d["spp"],
+                        max_depth=d["max_depth"], seed=d["seed"])
+
+
 def main():
     if not po.ref_available():
         raise SystemExit("oracle/_ref/libpolyref.so is not built; run `make -C oracle` where the reference is present")
+    if sys.argv[1:] == ["batch_box_scene"]:  # regenerate only this fixture
+        make_box_scene_fixture()
+        return
     check_unit_cases_against_ref()
     with open(os.path.join(HERE, "reference_unit_cases.json"), "w") as f:
         json.dump(UNIT_CASES, f, indent=1)
@@ -216,6 +255,7 @@ def main():
     rgb3, prim3 = ref3.render(inst)
     np.savez_compressed(os.path.join(HERE, "instanced_small.npz"), inputs_sha=scene_inputs_digest(im),
                         tree_sha=sha(n3, p3), num_nodes=len(n3), rgb=rgb3, prim=prim3)
+    make_box_scene_fixture()
     print("wrote fixtures:", sorted(f for f in os.listdir(HERE) if f.endswith((".npz", ".json"))))
 
 

@@ -147,3 +147,59 @@ def test_server_poisson_arrivals_latency(cuda_device):
         srv.fetch(t)
     assert np.percentile(lats, 99) >= np.percentile(lats, 50) > 0
     srv.close()
+
+
+def test_server_cancel_queued_and_in_flight_requests(cuda_device):
+    """pt_server_cancel: a queued request ends at once; an admitted one stops getting work and ends
+    after the waves already queued with its work; the others still finish with pt_render's films,
+    and every byte of device memory and host arena goes back.  A wait that runs out returns
+    PT_ETIMEOUT with the request's current state."""
+    jobs = small_jobs(4, seed=31)
+    meshes, env = W.instanced_scene(level=6, instances=3)
+    big_scene = pb.Scene(meshes, env)
+    big = pb.render_desc(1024, 1024, 16, 5, W.INSTANCED_CAMERA, 3, pb.RENDER_NEE)
+    t = pb.default_tuning()
+    t.pipeline = pb.PIPELINE_PATHS
+    # one request at a time, small waves: the big request spans hundreds of waves
+    srv = pb.Server(max_inflight=1, wave_pixels=1 << 16, tuning=t)
+    ta = srv.submit(big_scene, big)
+    others = [srv.submit(scene, rd) for scene, rd in jobs]
+    # a wait that runs out reports the timeout and the state so far
+    with pytest.raises(pb.PolytopeError) as e:
+        srv.wait(ta, 1)
+    assert e.value.code == pb.PT_ETIMEOUT
+    # the last queued request is cancelled while the big one runs
+    assert srv.poll(others[-1])[0] == pb.REQ_QUEUED
+    srv.cancel(others[-1])
+    assert srv.poll(others[-1])[0] == pb.REQ_CANCELLED
+    assert srv.wait(others[-1], 1000) == pb.REQ_CANCELLED
+    # the big request is cancelled once its first wave is queued
+    deadline = time.time() + 30
+    while srv.timing(ta)["first_wave_ms"] < 0 and time.time() < deadline:
+        time.sleep(0.001)
+    assert srv.poll(ta)[0] == pb.REQ_ADMITTED
+    srv.cancel(ta)
+    assert srv.wait(ta, 60000) == pb.REQ_CANCELLED
+    for tk, (scene, rd) in zip(others[:-1], jobs[:-1]):
+        assert srv.wait(tk, 60000) == pb.REQ_DONE
+        assert_bit_equal(srv.fetch(tk)[0], solo(scene, rd)[0], "film after a cancellation")
+    for tk in (ta, others[-1]):
+        with pytest.raises(pb.PolytopeError) as e:
+            srv.fetch(tk)
+        assert e.value.code == pb.PT_ECANCELED
+    s = srv.stats()
+    assert s["cancelled"] == 2 and s["completed"] == len(jobs) - 1
+    assert s["device_bytes_in_use"] == 0 and s["host_bytes_in_use"] == 0 and s["active"] == 0 and s["pending"] == 0
+    # the big request stopped early: far fewer waves than its 16,777,216 paths would take
+    assert s["waves"] < (1024 * 1024 * 16) >> 16
+    # cancelling a finished or unknown request is refused
+    tk = srv.submit(*jobs[0])
+    assert srv.wait(tk, 60000) == pb.REQ_DONE
+    with pytest.raises(pb.PolytopeError) as e:
+        srv.cancel(tk)
+    assert e.value.code == pb.PT_EINVAL
+    srv.fetch(tk)
+    with pytest.raises(pb.PolytopeError):
+        srv.cancel(10 ** 9)
+    srv.close()
+    big_scene.close()

@@ -174,6 +174,27 @@ def test_instanced_fixture():
     assert_bit_equal(prim, g["prim"], "prim")
 
 
+def test_batch_box_scene_fixture():
+    """Scene 12 of the 256-scene batched workload (icosphere among 104 boxes, 64x64, 64 spp, depth
+    6, NEE): tree, box corner/edge hits with per-ray counts and the whole film equal the
+    reference's."""
+    from golden.make_golden import BOX_SCENE_INDEX
+    g = load_golden("batch_box_scene.npz")
+    meshes, env, d = W.batched_workload(256)[BOX_SCENE_INDEX]
+    assert scene_inputs_digest(meshes) == str(g["inputs_sha"])
+    s = po.OracleScene(meshes, env)
+    nodes, pairs = s.tree()
+    assert sha(nodes, pairs) == str(g["tree_sha"])
+    hits, nt, tt = s.trace(g["rays"], counts=True)
+    for f in ("prim", "t", "u", "v"):
+        assert_bit_equal(hits[f], g["hits"][f], f)
+    assert_bit_equal(nt, g["node_tests"], "nodes")
+    assert_bit_equal(tt, g["tri_tests"], "tris")
+    rgb, prim = s.render(dict(d, flags=1))
+    assert_bit_equal(rgb, g["rgb"], "rgb")
+    assert_bit_equal(prim, g["prim"], "prim")
+
+
 @pytest.mark.skipif(not po.ref_available(), reason="oracle/_ref is only built where the reference tree is present")
 def test_oracle_matches_reference_on_random_multimesh_scene():
     rng = np.random.default_rng(7)

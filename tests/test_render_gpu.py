@@ -172,3 +172,12 @@ def test_film_to_rgba8_matches_reference_quantisation(cuda_device):
     torch.cuda.synchronize()
     host_film = film.cpu().numpy().reshape(48, 64, 3)
     assert_bit_equal(pb.film_to_rgba8(film.data_ptr(), 64, 48), po.film_to_rgba8(host_film), "rendered film")
+    # the render call with the output step on the device: host bytes, and device bytes queued on a stream
+    rgba, prim = pb.render_rgba8(scene, 64, 48, 4, 4, W.SMALL_CAMERA, 5, pb.RENDER_NEE)
+    assert_bit_equal(rgba, po.film_to_rgba8(host_film), "pt_render_rgba8 host")
+    assert_bit_equal(prim, pb.render(scene, 64, 48, 4, 4, W.SMALL_CAMERA, 5, pb.RENDER_NEE)[1], "pt_render_rgba8 prim")
+    dbytes = torch.zeros(64 * 48 * 4, dtype=torch.uint8, device="cuda")
+    st = torch.cuda.Stream()
+    pb.check(pb.lib.pt_render_rgba8(scene.handle, C.byref(rd), dbytes.data_ptr(), None, pb.MEM_DEVICE, st.cuda_stream))
+    assert scene.status(st.cuda_stream) == pb.PT_OK
+    assert_bit_equal(dbytes.cpu().numpy().reshape(48, 64, 4), po.film_to_rgba8(host_film), "pt_render_rgba8 device")
