@@ -278,6 +278,7 @@ def run_served(pb, srv, scenes, reqs, arrivals, films=None):
     films = films or film_buffers(reqs)
     rays0 = srv.stats()["rays_traced"]
     lats = np.zeros(len(reqs))
+    run_served.admission_ms = adm = np.zeros(len(reqs))  # submission -> admission, per request
     q = queue.Queue()
 
     def client():
@@ -285,6 +286,7 @@ def run_served(pb, srv, scenes, reqs, arrivals, films=None):
             t = q.get()
             srv.wait(t, 600000)
             lats[k] = srv.poll(t)[1]
+            adm[k] = srv.timing(t)["admitted_ms"]
             rd = reqs[k][1]
             pb.check(pb.lib.pt_server_fetch(srv.handle, t, films[rd.width * rd.height].ctypes.data, None))
 
@@ -371,6 +373,7 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
             served[-1]["gpu_busy_ms"] = round(s1["busy_ms"] - s0["busy_ms"], 1)
             served[-1]["waves"] = int(s1["waves"] - s0["waves"])
             served[-1]["blocked_admission_ms"] = round(s1["blocked_ms"] - s0["blocked_ms"], 1)
+            served[-1]["admission_wait_ms"] = {"p50": pct(run_served.admission_ms, 50), "p99": pct(run_served.admission_ms, 99)}
             lat_p, span_p = run_plain(pb, scenes, reqs, arrivals, films)
             plain.append(summary(lat_p, span_p, rays))
             if top:
@@ -399,7 +402,11 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
     s1 = bsrv.stats()
     out["memory_budgeted"] = dict(summary(lat_b, span_b, rays_b), rate_per_s=max(rates), memory_budget_bytes=budget,
                                   blocked_admission_ms=round(s1["blocked_ms"] - s0["blocked_ms"], 1),
-                                  gpu_busy_ms=round(s1["busy_ms"] - s0["busy_ms"], 1))
+                                  admission_wait_ms={"p50": pct(run_served.admission_ms, 50),
+                                                     "p99": pct(run_served.admission_ms, 99)},
+                                  gpu_busy_ms=round(s1["busy_ms"] - s0["busy_ms"], 1),
+                                  note="blocked_admission_ms counts scheduler time idle with requests queued and no room; "
+                                       "admission_wait_ms is each request's submission-to-admission time")
     bsrv.close()
     return out
 
@@ -511,8 +518,8 @@ def main():
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-render", action="store_true")
     ap.add_argument("--render-probe", action="store_true",
-                    help="render the instanced scene at 480x270, 16 spp once with the plain launch and once with "
-                         "the persistent path kernel, then exit (a small case for profilers)")
+                    help="render the instanced scene at 480x270, 16 spp once with the fused kernel (PT_RENDER_FUSED) "
+                         "and once with pt_render's default persistent path kernel, then exit (a small case for profilers)")
     ap.add_argument("--batch-probe", action="store_true",
                     help="run the first 32 scenes of the 256-scene batch once through the wavefront pipeline with "
                          "the tuning the autotuner picks for the full batch, then exit (a small case for profilers)")
@@ -531,7 +538,7 @@ def main():
         meshes, env = W.instanced_scene()
         scene = pb.Scene(meshes, env)
         d = W.INSTANCED_RENDER
-        for fl in (0, pb.RENDER_PERSISTENT):
+        for fl in (pb.RENDER_FUSED, 0):
             rgb, _ = pb.render(scene, 480, 270, 16, d["max_depth"], d["camera"], d["seed"], pb.RENDER_NEE | fl)
             print(json.dumps({"render_probe": "480x270x16", "flags": pb.RENDER_NEE | fl, "mean": float(rgb.mean())}))
         return

@@ -239,8 +239,31 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WfItem* __restrict_
 // (with the voted walk: 1706 Msamples/s; 8: 1545, 12: 1640, 24: 1603).
 constexpr int kShadeBatch = 16;
 
-// 8 blocks of 128 per SM (64 registers, the rest spilled) measured fastest with the warp-voted
-// walk on the 6.5 M-face frame: 1700 Msamples/s against 1668 at 7 blocks, 1651 at 6, 1637 at 9.
+// Per-lane path state that only the shading step reads or writes (the path's next ray, throughput,
+// radiance, bounce count, the pending shadow contribution, the slot and its pixel, sample and
+// item), parked in shared memory between shading steps: the walk loop then holds only the ray
+// walk and the scene pointers in registers, so it runs at 8 blocks per SM without spilling its
+// state to local memory.  Field f of lane t lives at [f * 128 + t] (consecutive lanes, consecutive
+// banks).
+enum ColdField : uint32_t {
+    kOx, kOy, kOz, kDx, kDy, kDz, kSr, kSg, kSb, kLr, kLg, kLb, kCr, kCg, kCb,
+    kBounces, kFlags, kSlot, kPixel, kSample, kItem, kColdFields
+};
+constexpr uint32_t kColdShadow = 1u, kColdPending = 2u, kColdLambert = 4u;
+
+struct ColdLane {
+    uint32_t* c;  // this lane's field 0
+    __device__ __forceinline__ float f(uint32_t k) const { return __uint_as_float(c[k * 128]); }
+    __device__ __forceinline__ uint32_t u(uint32_t k) const { return c[k * 128]; }
+    __device__ __forceinline__ void set(uint32_t k, float v) const { c[k * 128] = __float_as_uint(v); }
+    __device__ __forceinline__ void set(uint32_t k, uint32_t v) const { c[k * 128] = v; }
+    __device__ __forceinline__ F3 f3at(uint32_t k) const { return f3(f(k), f(k + 1), f(k + 2)); }
+    __device__ __forceinline__ void set3(uint32_t k, const F3& v) const { set(k, v.x); set(k + 1, v.y); set(k + 2, v.z); }
+};
+
+// 8 blocks of 128 per SM with the shading state in shared memory (see ColdField): on the 6.5 M-face
+// 1920x1080x64 frame 1840-1847 Msamples/s against 1794-1796 with that state in registers (and
+// spilled), and 1678 against 1584 Mrays/s on the 256-scene batch.
 template <int CAP, int SH>
 __global__ void __launch_bounds__(128, 8) wf_path_kernel(const WfItem* __restrict__ items, const WfSegment* __restrict__ segs,
                                                       uint32_t nseg, uint32_t count, float* __restrict__ radiance,
@@ -250,18 +273,16 @@ __global__ void __launch_bounds__(128, 8) wf_path_kernel(const WfItem* __restric
     const uint32_t lt_mask = (1u << lane) - 1u;
     const float inf = bitsf(0x7F800000u);
     __shared__ uint32_t sstack[SH > 0 ? SH * 128 : 1];
+    __shared__ uint32_t scold[kColdFields * 128];
+    const ColdLane cold{scold + threadIdx.x};
     RayWalkT<CAP, SH> k;
     k.stack.base = sstack + threadIdx.x;
     k.stack.stride = 128;
-    uint64_t pool_next = 0, pool_end = 0;
-    bool exhausted = false, active = false, shadow = false, pending = false;
-    uint32_t slot = 0, pixel = 0, sample = 0, num_nodes = 0, rays = 0;
-    const RenderParams* p = nullptr;
-    uint32_t* primary = nullptr;
+    uint32_t pool_next = 0, pool_end = 0;
+    bool exhausted = false, active = false;
+    uint32_t num_nodes = 0, rays = 0;
     const uint4* nodes = nullptr;
     const float4* tris = nullptr;
-    PathState s;
-    F3 contrib = f3(0.f, 0.f, 0.f);
     bool finished = false, walk_ok = true;  // the current ray's walk has ended (and how)
     while (true) {
         const uint32_t need = __ballot_sync(0xFFFFFFFFu, !active);
@@ -272,33 +293,39 @@ __global__ void __launch_bounds__(128, 8) wf_path_kernel(const WfItem* __restric
             if (base >= count) {
                 exhausted = true;
             } else {
-                pool_next = base;
-                pool_end = base + chunk < count ? base + chunk : count;
+                pool_next = (uint32_t)base;
+                pool_end = base + chunk < count ? (uint32_t)base + chunk : count;
             }
         }
         if (need) {
-            const uint64_t avail = pool_end - pool_next;
+            const uint32_t avail = pool_end - pool_next;
             const uint32_t rank = __popc(need & lt_mask);
             if (!active && rank < avail) {
-                slot = (uint32_t)(pool_next + rank);
+                const uint32_t slot = pool_next + rank;
                 const WfSegment sg = segs[find_segment(segs, nseg, slot)];
-                const WfItem& it = items[sg.item];
-                p = it.params;
-                primary = it.primary;
+                const uint32_t item = sg.item;
+                const RenderParams* p = items[item].params;
                 nodes = (const uint4*)p->nodes;
                 tris = (const float4*)p->tris;
                 num_nodes = p->num_nodes;
-                path_camera(*p, sg.local_begin + (slot - sg.slot_base), pixel, sample, s.o, s.d);
-                s.src = f3(1.f, 1.f, 1.f);
-                s.L = f3(0.f, 0.f, 0.f);
-                s.bounces = 0;
-                s.last_lambert = 0;
-                shadow = false;
-                walk_begin(k, s.o.x, s.o.y, s.o.z, s.d.x, s.d.y, s.d.z, inf, false);
+                uint32_t pixel, sample;
+                F3 o, d;
+                path_camera(*p, sg.local_begin + (slot - sg.slot_base), pixel, sample, o, d);
+                cold.set3(kOx, o);
+                cold.set3(kDx, d);
+                cold.set3(kSr, f3(1.f, 1.f, 1.f));
+                cold.set3(kLr, f3(0.f, 0.f, 0.f));
+                cold.set(kBounces, 0u);
+                cold.set(kFlags, 0u);
+                cold.set(kSlot, slot);
+                cold.set(kPixel, pixel);
+                cold.set(kSample, sample);
+                cold.set(kItem, item);
+                walk_begin(k, o.x, o.y, o.z, d.x, d.y, d.z, inf, false);
                 active = true;
                 finished = false;
             }
-            const uint64_t took = (uint64_t)__popc(need) < avail ? (uint64_t)__popc(need) : avail;
+            const uint32_t took = (uint32_t)__popc(need) < avail ? (uint32_t)__popc(need) : avail;
             pool_next += took;
         }
         if (!__any_sync(0xFFFFFFFFu, active)) {
@@ -309,7 +336,6 @@ __global__ void __launch_bounds__(128, 8) wf_path_kernel(const WfItem* __restric
             uint32_t leaf_off = 0, leaf_n = 0;
             bool ok, at_leaf;
             if constexpr (PT_LEAF_BATCH_PATHS > 0) {
-                // one node step per ballot: two measured 3 % slower here (1651 vs 1707 Msamples/s)
                 walk_round<false, 1>(k, active && !finished && k.sp > 0, PT_LEAF_BATCH_PATHS, nodes, num_nodes, at_leaf,
                                      ok, leaf_off, leaf_n);
             } else {
@@ -328,33 +354,52 @@ __global__ void __launch_bounds__(128, 8) wf_path_kernel(const WfItem* __restric
         if (fin && (walking == 0 || __popc(fin) >= kShadeBatch)) {
             if (active && finished) {
                 finished = false;
-                const bool ok = walk_ok;
                 ++rays;
-                bool go = false;
-                if (!ok) {
+                const WfItem& it = items[cold.u(kItem)];
+                const RenderParams* p = it.params;
+                uint32_t flags = cold.u(kFlags);
+                const bool shadow = (flags & kColdShadow) != 0;
+                bool go = false, next_shadow = false;
+                if (!walk_ok) {
                     raise_flag(p->err);
                 } else if (!shadow) {
-                    if (s.bounces == 0 && sample == 0 && primary) primary[pixel] = k.prim;
+                    PathState s;
+                    s.o = cold.f3at(kOx);
+                    s.d = cold.f3at(kDx);
+                    s.src = cold.f3at(kSr);
+                    s.L = cold.f3at(kLr);
+                    s.bounces = cold.u(kBounces);
+                    s.last_lambert = (flags & kColdLambert) ? 1u : 0u;
+                    const uint32_t pixel = cold.u(kPixel), sample = cold.u(kSample);
+                    if (s.bounces == 0 && sample == 0 && it.primary) it.primary[pixel] = k.prim;
                     ShadowReq sh;
                     const bool more = shade_hit(*p, s, k.prim, k.leaf, k.u, k.v, k.w, pixel, sample, sh);
+                    cold.set3(kOx, s.o);
+                    cold.set3(kDx, s.d);
+                    cold.set3(kSr, s.src);
+                    cold.set3(kLr, s.L);
+                    cold.set(kBounces, s.bounces);
+                    flags = s.last_lambert ? kColdLambert : 0u;
                     if (sh.valid) {
-                        contrib = sh.contrib;
-                        pending = more;
-                        shadow = true;
+                        cold.set3(kCr, sh.contrib);
+                        flags |= kColdShadow | (more ? kColdPending : 0u);
+                        next_shadow = true;
                         walk_begin(k, sh.o.x, sh.o.y, sh.o.z, sh.wi.x, sh.wi.y, sh.wi.z, sh.tmax, true);
                     } else {
-                        go = more;
+                        go = more && !throughput_is_zero(s.src);
                     }
+                    cold.set(kFlags, flags);
                 } else {
-                    if (k.prim == kPrimNone) s.L = vadd(s.L, contrib);
-                    shadow = false;
-                    go = pending;
+                    if (k.prim == kPrimNone) cold.set3(kLr, vadd(cold.f3at(kLr), cold.f3at(kCr)));
+                    go = (flags & kColdPending) != 0 && !throughput_is_zero(cold.f3at(kSr));
+                    cold.set(kFlags, flags & ~(kColdShadow | kColdPending));
                 }
-                if (!shadow) {
-                    if (go && !throughput_is_zero(s.src)) {
-                        walk_begin(k, s.o.x, s.o.y, s.o.z, s.d.x, s.d.y, s.d.z, inf, false);
+                if (!next_shadow) {
+                    if (go) {
+                        const F3 o = cold.f3at(kOx), d = cold.f3at(kDx);
+                        walk_begin(k, o.x, o.y, o.z, d.x, d.y, d.z, inf, false);
                     } else {
-                        clamp_store(radiance + 3 * (size_t)slot, s.L);
+                        clamp_store(radiance + 3 * (size_t)cold.u(kSlot), cold.f3at(kLr));
                         active = false;
                     }
                 }

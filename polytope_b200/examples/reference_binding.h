@@ -92,7 +92,9 @@ inline int describe_scene(poly::Scene &scene, scene_desc &out, bool keep_tree) {
          o.albedo[0] = r->refl.r;
          o.albedo[1] = r->refl.g;
          o.albedo[2] = r->refl.b;
-      } else if (!o.is_light) {
+      } else if (o.is_light) {
+         o.material = PT_MAT_LAMBERT;  // an emitter's material is never sampled (the path ends there)
+      } else {
          return PT_EINVAL;
       }
    }
