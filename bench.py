@@ -196,6 +196,19 @@ def bench_render(pb, torch, cpu=True, cpu_rows=16, threads=None):
     film = out.view(rd.height, rd.width, 3).cpu().numpy()
     prim_ids = prim.view(rd.height, rd.width).cpu().numpy().view(np.uint32)
     assert scene.status() == pb.PT_OK
+    # the same frame on the two-level (instanced) layout: one copy of the sphere instead of five
+    two = pb.Scene(meshes, env, two_level=True)
+    two_ms = timed(lambda: pb.check(pb.lib.pt_render(two.handle, C.byref(rd), out.data_ptr(), prim.data_ptr(),
+                                                     pb.MEM_DEVICE, None)))
+    two_film = out.view(rd.height, rd.width, 3).cpu().numpy().astype(np.float64)
+    two_prim = prim.view(rd.height, rd.width).cpu().numpy().view(np.uint32)
+    f64 = film.astype(np.float64)
+    two_level = {"ms": round(two_ms, 2), "msamples_s": round(samples / two_ms / 1e3, 1), "pipeline": "fused (two-level scenes)",
+                 "device_bytes": int(two.info().device_bytes), "flattened_device_bytes": int(scene.info().device_bytes),
+                 "memory_ratio": round(scene.info().device_bytes / two.info().device_bytes, 2),
+                 "rel_rmse_vs_flattened": float(np.sqrt(((two_film - f64) ** 2).mean()) / np.sqrt((f64 ** 2).mean())),
+                 "primary_ids_equal_frac": float((two_prim == prim_ids).mean())}
+    two.close()
     best, _, trials = pb.autotune([(scene, rd)])
     b = pb.Batch([(scene, rd)], best)
     tuned_ms = timed(b.run)
@@ -211,6 +224,7 @@ def bench_render(pb, torch, cpu=True, cpu_rows=16, threads=None):
                            "film_equals_plain": bool(np.array_equal(fused_film.view(np.uint32), film.view(np.uint32)))},
            "autotuned": {"ms": round(tuned_ms, 2), "msamples_s": round(samples / tuned_ms / 1e3, 1),
                          "mrays_s": round(rays / tuned_ms / 1e3, 1), "tuning": best.as_dict(), "trials": len(trials)},
+           "two_level": two_level,
            "autotuned_equals_plain": bool(np.array_equal(tuned_film.view(np.uint32), film.view(np.uint32))
                                           and np.array_equal(tuned_prim, prim_ids)),
            "timing": "CUDA events, median of 3 after one warm-up; films stay on the device"}
@@ -335,8 +349,12 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
     """Resident scene pool, Poisson request arrivals at each rate: the serving loop vs one
     pt_render per request in arrival order.  Latency = completion - arrival."""
     from polytope_b200 import workloads as W
-    scenes = build_scenes(pb, W.serving_pool(n_scenes))
+    pool = W.serving_pool(n_scenes)
+    scenes = build_scenes(pb, pool)
     reqs, unit = serve_requests(pb, n_scenes, n_requests, seed)
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(8) as ex:
+        two_bytes = sum(ex.map(lambda sp: pb.two_level_plan(sp[0], sp[1])["device_bytes"], pool))
     # one long-running service for every rate; both arms are warmed on the whole request list
     # (memory pools, host arena, lazily loaded kernels), submitted at once
     srv = make_server(pb)
@@ -351,7 +369,10 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
                      "into reused buffers (the plain arm renders into the same reused buffers)",
            "timing": "host steady clock from the first arrival to the last completion (film in host memory); latency = completion - arrival; "
                      "each arm's run with the median makespan of 3 (runs: [Mrays/s, p99 ms(, GPU busy ms of the waves)] of each)",
-           "rates": []}
+           "rates": [],
+           "pool": {"faces": int(sum(sum(len(m.faces) for m in sp[0]) for sp in pool)),
+                    "device_bytes": int(sum(sc.info().device_bytes for sc in scenes)),
+                    "two_level_device_bytes": int(two_bytes)}}
     def summary(lat, span, rays):
         return {"mrays_s": round(rays / span / 1e6, 1), "p50_ms": pct(lat, 50), "p95_ms": pct(lat, 95),
                 "p99_ms": pct(lat, 99), "makespan_s": round(span, 3)}

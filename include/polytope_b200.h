@@ -116,6 +116,35 @@ int pt_bvh_build(const pt_mesh_desc *meshes, uint32_t num_meshes, int threads,
 /* Upload a scene to the current CUDA device.  The descriptor's arrays are copied; the caller may
  * free them on return. */
 int pt_scene_create(const pt_scene_desc *desc, pt_scene **out);
+/* Two-level (instanced) scene: an opt-in layout with no counterpart in the reference, which
+ * flattens every ObjectInstance into its own world-space mesh and one tree
+ * (src/common/parsers/pbrt_parser.cpp:1439-1472, bvh::bound src/cpu/acceleration/bvh.cpp:36-130).
+ * Meshes of `desc` whose vertex, face and normal arrays are the same pointers with the same counts
+ * share one geometry: it is stored once, in object space, with its own tree (the same SAH build);
+ * each mesh becomes an instance with its object_to_world (affine and invertible), and a top-level
+ * tree over the instances' world boxes picks the instances a ray reaches.  Rays are carried into
+ * object space for the bottom-level tests, so hits are those of the flattened scene up to float
+ * rounding: primitive ids agree wherever the first hit is unambiguous, t to about 1e-6 relative,
+ * and images agree in RMSE rather than bit for bit.  Shading uses the instance's world vertices
+ * computed as pt_scene_create bakes them.  Primitive ids, materials, lights and the environment
+ * are the flattened scene's.  The scene works with pt_trace / pt_trace_counted (node counts then
+ * include top-level tests), pt_render and pt_render_rgba8 with the fused pipeline (the default
+ * for such scenes; PT_RENDER_PERSISTENT and PT_RENDER_WAVEFRONT are rejected), pt_render_noalloc,
+ * and batches and servers with PT_PIPELINE_FUSED.  `desc->nodes` must be NULL. */
+int pt_scene_create_two_level(const pt_scene_desc *desc, pt_scene **out);
+
+/* What pt_scene_create_two_level would build from `desc`, computed on the host alone (no device
+ * needed): counts and the device bytes the scene would hold. */
+typedef struct pt_two_level_info {
+    uint32_t num_instances, num_geometries;
+    uint32_t blas_nodes, blas_faces;    /* bottom-level trees and faces, all geometries   */
+    uint32_t tlas_nodes;
+    uint32_t max_depth, tlas_depth;      /* deepest bottom-level and top-level node         */
+    uint32_t num_prims;                  /* faces of the flattened scene (primitive ids)    */
+    uint64_t device_bytes;
+} pt_two_level_info;
+int pt_two_level_plan(const pt_scene_desc *desc, pt_two_level_info *info);
+
 int pt_scene_destroy(pt_scene *scene);
 
 typedef struct pt_scene_info {

@@ -162,6 +162,7 @@ def _load() -> C.CDLL:
         "pt_version": (C.c_char_p, []),
         "pt_bvh_build": (i, [C.POINTER(MeshDesc), u32, i, _vp, _up, _up]),
         "pt_scene_create": (i, [C.POINTER(SceneDesc), C.POINTER(_vp)]),
+        "pt_scene_create_two_level": (i, [C.POINTER(SceneDesc), C.POINTER(_vp)]),
         "pt_scene_destroy": (i, [_vp]),
         "pt_scene_get_info": (i, [_vp, C.POINTER(SceneInfo)]),
         "pt_trace": (i, [_vp, _vp, u64, _vp, u32, _vp]),
@@ -268,19 +269,29 @@ class Mesh:
 
 
 def mesh_descs(meshes: Sequence[Mesh]):
-    """ctypes array of MeshDesc (same layout as pt_mesh_desc) plus the arrays it points into."""
+    """ctypes array of MeshDesc (same layout as pt_mesh_desc) plus the arrays it points into.
+    Meshes built on the same face (and normal) arrays get the same column arrays, so their
+    descriptors share every geometry pointer (what pt_scene_create_two_level keys instances on)."""
     arr = (MeshDesc * len(meshes))()
     keep = []
+    columns = {}
+
+    def cols(a, dtype):
+        key = (a.__array_interface__["data"][0], a.shape, a.strides, np.dtype(dtype).str)
+        if key not in columns:
+            c = np.ascontiguousarray(a, dtype)
+            columns[key] = tuple(np.ascontiguousarray(c[:, j]) for j in range(3))
+            keep.extend(columns[key])
+        return columns[key]
+
     for k, m in enumerate(meshes):
-        f0, f1, f2 = (np.ascontiguousarray(m.faces[:, j]) for j in range(3))
-        keep += [m.x, m.y, m.z, f0, f1, f2]
+        f0, f1, f2 = cols(m.faces, np.uint32)
+        keep += [m.x, m.y, m.z]
         d = arr[k]
         d.x, d.y, d.z, d.num_vertices = _f(m.x), _f(m.y), _f(m.z), len(m.x)
         d.fv0, d.fv1, d.fv2, d.num_faces = _u(f0), _u(f1), _u(f2), len(f0)
         if m.normals is not None:
-            n = np.ascontiguousarray(m.normals, np.float32)
-            nx, ny, nz = (np.ascontiguousarray(n[:, j]) for j in range(3))
-            keep += [nx, ny, nz]
+            nx, ny, nz = cols(m.normals, np.float32)
             d.nx, d.ny, d.nz = _f(nx), _f(ny), _f(nz)
         d.object_to_world[:] = [float(v) for v in m.object_to_world.ravel()]
         d.world_to_object[:] = [float(v) for v in m.world_to_object.ravel()]
@@ -303,6 +314,44 @@ def bvh_build(meshes: Sequence[Mesh], threads: int = 0):
     return nodes[:n.value].copy(), pairs
 
 
+def scene_desc(meshes: Sequence[Mesh], env=None, nodes=None, leaf_pairs=None):
+    """pt_scene_desc of the meshes (plus the arrays it points into, to keep alive)."""
+    arr, keep = mesh_descs(meshes)
+    d = SceneDesc()
+    d.meshes = arr
+    d.num_meshes = len(meshes)
+    keep.append(arr)
+    if nodes is not None:
+        nodes = np.ascontiguousarray(nodes, NODE_DTYPE)
+        pairs = np.ascontiguousarray(leaf_pairs, np.uint32)
+        keep += [nodes, pairs]
+        d.nodes = nodes.ctypes.data
+        d.num_nodes = len(nodes)
+        d.leaf_pairs = _u(pairs)
+    d.has_env = int(env is not None)
+    if env is not None:
+        d.env[:] = [float(v) for v in env]
+    return d, keep
+
+
+class TwoLevelInfo(C.Structure):
+    _fields_ = [("num_instances", C.c_uint32), ("num_geometries", C.c_uint32), ("blas_nodes", C.c_uint32),
+                ("blas_faces", C.c_uint32), ("tlas_nodes", C.c_uint32), ("max_depth", C.c_uint32),
+                ("tlas_depth", C.c_uint32), ("num_prims", C.c_uint32), ("device_bytes", C.c_uint64)]
+
+
+lib.pt_two_level_plan.restype = C.c_int
+lib.pt_two_level_plan.argtypes = [C.POINTER(SceneDesc), C.POINTER(TwoLevelInfo)]
+
+
+def two_level_plan(meshes: Sequence[Mesh], env=None) -> dict:
+    """pt_two_level_plan: what a two-level scene of these meshes would hold (host only)."""
+    d, keep = scene_desc(list(meshes), env)
+    info = TwoLevelInfo()
+    check(lib.pt_two_level_plan(C.byref(d), C.byref(info)))
+    return {k: int(getattr(info, k)) for k, _ in info._fields_}
+
+
 def _ptr(a) -> int:
     """Address of a numpy array or a torch tensor (device pointers for MEM_DEVICE calls)."""
     if hasattr(a, "data_ptr"):
@@ -314,24 +363,15 @@ class Scene:
     """poly::Scene on the GPU: meshes (Shapes and Lights), optional constant environment, BVH."""
 
     def __init__(self, meshes: Sequence[Mesh], env: Optional[Sequence[float]] = None,
-                 nodes: Optional[np.ndarray] = None, leaf_pairs: Optional[np.ndarray] = None):
+                 nodes: Optional[np.ndarray] = None, leaf_pairs: Optional[np.ndarray] = None,
+                 two_level: bool = False):
+        """two_level: pt_scene_create_two_level -- meshes sharing their vertex and face arrays
+        become instances of one object-space geometry under a top-level tree."""
         self.meshes = list(meshes)
-        arr, keep = mesh_descs(self.meshes)
-        d = SceneDesc()
-        d.meshes = arr
-        d.num_meshes = len(self.meshes)
-        if nodes is not None:
-            nodes = np.ascontiguousarray(nodes, NODE_DTYPE)
-            pairs = np.ascontiguousarray(leaf_pairs, np.uint32)
-            keep += [nodes, pairs]
-            d.nodes = nodes.ctypes.data
-            d.num_nodes = len(nodes)
-            d.leaf_pairs = _u(pairs)
-        d.has_env = int(env is not None)
-        if env is not None:
-            d.env[:] = [float(v) for v in env]
+        self.two_level = two_level
+        d, keep = scene_desc(self.meshes, env, nodes, leaf_pairs)
         h = _vp()
-        check(lib.pt_scene_create(C.byref(d), C.byref(h)))
+        check((lib.pt_scene_create_two_level if two_level else lib.pt_scene_create)(C.byref(d), C.byref(h)))
         self.handle = h
         self.prim_base = np.concatenate([[0], np.cumsum([len(m.faces) for m in self.meshes])]).astype(np.int64)
 

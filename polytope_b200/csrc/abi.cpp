@@ -58,7 +58,8 @@ void free_scene(pt_scene* s) {
     if (!s) return;
     DeviceGuard g(s->device);
     void* bufs[] = {s->dev.nodes, s->dev.tris, s->dev.meshes, s->dev.prim_normals, s->dev.prim_tri,
-                    s->dev.light_tris, s->dev.light_cdf, s->dev_in, s->dev_out, s->err_flag, s->trace_err, s->ray_counters};
+                    s->dev.light_tris, s->dev.light_cdf, s->dev.instances, s->dev.tlas_nodes, s->dev_in, s->dev_out,
+                    s->err_flag, s->trace_err, s->ray_counters};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (s->pin_in) cudaFreeHost(s->pin_in);
@@ -124,6 +125,9 @@ int scene_trace(pt_scene* s, const pt_ray* rays, uint64_t n, pt_hit* hits, uint3
     a.err = (int*)s->err_flag;
     a.shared_stack = (int)s->trace_tuning.shared_stack;
     a.chunk = s->trace_tuning.queue_chunk;
+    a.instances = s->dev.instances;
+    a.top_nodes = s->dev.tlas_nodes;
+    a.top_num_nodes = s->dev.tlas_num_nodes;
     auto next_counter = [s]() {
         return (void*)((unsigned long long*)s->ray_counters + (s->counter_next.fetch_add(1) % PT_RAY_COUNTERS));
     };
@@ -267,6 +271,11 @@ int prepare_scene_host(const pt_scene_desc* desc, HostScene& h) {
         o[9] = bitsf(p);
         o[10] = bitsf(m);
     }
+    prepare_shading_host(desc, w, h);
+    return PT_OK;
+}
+
+void prepare_shading_host(const pt_scene_desc* desc, const WorldMeshes& w, HostScene& h) {
     h.meshes.resize(desc->num_meshes);
     bool any_normals = false;
     for (uint32_t m = 0; m < desc->num_meshes; ++m) {
@@ -313,7 +322,6 @@ int prepare_scene_host(const pt_scene_desc* desc, HostScene& h) {
         h.light_tris.push_back(0.f);
         h.light_cdf.push_back(h.light_area);
     }
-    return PT_OK;
 }
 
 }  // namespace pt
@@ -346,18 +354,22 @@ int pt_bvh_build(const pt_mesh_desc* meshes, uint32_t num_meshes, int threads, p
     return PT_OK;
 }
 
-int pt_scene_create(const pt_scene_desc* desc, pt_scene** out) {
-    if (!desc || !out) return fail(PT_EINVAL, "desc or out is NULL");
-    *out = nullptr;
+}  // extern "C"
+
+namespace {
+int device_count_ok() {
     int ndev = 0;
     cudaError_t ce = cudaGetDeviceCount(&ndev);
     if (ce != cudaSuccess || ndev == 0) {
         cudaGetLastError();
         return fail(PT_ECUDA, "no CUDA device available (there is no CPU fallback)");
     }
-    HostScene h;
-    int rc = prepare_scene_host(desc, h);
-    if (rc) return rc;
+    return PT_OK;
+}
+
+// Uploads a prepared scene (either layout) into a new handle.
+int create_from_host(const pt_scene_desc* desc, HostScene& h, pt_scene** out) {
+    int rc = PT_OK;
     std::unique_ptr<pt_scene> s(new pt_scene());
     cudaGetDevice(&s->device);
     s->num_nodes = (uint32_t)h.nodes.size();
@@ -382,8 +394,61 @@ int pt_scene_create(const pt_scene_desc* desc, pt_scene** out) {
     if (cudaMalloc(&s->err_flag, sizeof(int)) != cudaSuccess) { free_scene(s.release()); return fail(PT_ENOMEM, "cudaMalloc error flag"); }
     cudaMemset(s->err_flag, 0, sizeof(int));
     if (cudaMalloc(&s->ray_counters, 8 * PT_RAY_COUNTERS) != cudaSuccess) { free_scene(s.release()); return fail(PT_ENOMEM, "cudaMalloc ray counters"); }
+    if (h.two_level) {
+        s->two_level = true;
+        s->dev.num_instances = (uint32_t)h.instances.size();
+        s->dev.tlas_num_nodes = (uint32_t)h.tlas.size();
+        if ((rc = upload(&s->dev.instances, h.instances.data(), h.instances.size(), bytes))) { free_scene(s.release()); return rc; }
+        if ((rc = upload(&s->dev.tlas_nodes, h.tlas.data(), h.tlas.size(), bytes))) { free_scene(s.release()); return rc; }
+    }
     s->device_bytes = bytes;
     *out = s.release();
+    return PT_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int pt_scene_create(const pt_scene_desc* desc, pt_scene** out) {
+    if (!desc || !out) return fail(PT_EINVAL, "desc or out is NULL");
+    *out = nullptr;
+    int rc = device_count_ok();
+    if (rc) return rc;
+    HostScene h;
+    rc = prepare_scene_host(desc, h);
+    if (rc) return rc;
+    return create_from_host(desc, h, out);
+}
+
+int pt_scene_create_two_level(const pt_scene_desc* desc, pt_scene** out) {
+    if (!desc || !out) return fail(PT_EINVAL, "desc or out is NULL");
+    *out = nullptr;
+    int rc = device_count_ok();
+    if (rc) return rc;
+    HostScene h;
+    rc = prepare_two_level_host(desc, h);
+    if (rc) return rc;
+    if (h.tlas_depth + 2 > (uint32_t)PT_TOP_STACK) return fail(PT_ESTACK, "top-level tree too deep");
+    return create_from_host(desc, h, out);
+}
+
+int pt_two_level_plan(const pt_scene_desc* desc, pt_two_level_info* info) {
+    if (!desc || !info) return fail(PT_EINVAL, "desc or info is NULL");
+    HostScene h;
+    int rc = prepare_two_level_host(desc, h);
+    if (rc) return rc;
+    info->num_instances = (uint32_t)h.instances.size();
+    info->num_geometries = h.num_geometries;
+    info->blas_nodes = (uint32_t)h.nodes.size();
+    info->blas_faces = (uint32_t)(h.tris.size() / 12);
+    info->tlas_nodes = (uint32_t)h.tlas.size();
+    info->max_depth = h.max_depth;
+    info->tlas_depth = h.tlas_depth;
+    info->num_prims = h.num_prims;
+    info->device_bytes = sizeof(pt_bvh_node) * (uint64_t)h.nodes.size() + 4ull * h.tris.size() +
+                         sizeof(DeviceMesh) * (uint64_t)h.meshes.size() + 4ull * h.normals.size() +
+                         4ull * h.light_tris.size() + 4ull * h.light_cdf.size() +
+                         sizeof(DeviceInstance) * (uint64_t)h.instances.size() + sizeof(pt_bvh_node) * (uint64_t)h.tlas.size();
     return PT_OK;
 }
 

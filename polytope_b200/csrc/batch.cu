@@ -23,7 +23,7 @@
 
 namespace pt {
 
-template <int CAP>
+template <int CAP, bool TWO_LEVEL>
 __global__ void __launch_bounds__(256) batch_kernel(const BatchItem* __restrict__ items, uint32_t n_items, uint64_t first,
                                                     uint64_t count, unsigned long long* counter, uint32_t chunk,
                                                     unsigned long long* rays_traced) {
@@ -77,7 +77,7 @@ __global__ void __launch_bounds__(256) batch_kernel(const BatchItem* __restrict_
         }
         if (active) {
             float L[3];
-            rays += path_fused<CAP>(*p, (uint64_t)sample * npix + px, L, sample == 0 ? it->primary : nullptr);
+            rays += path_fused<CAP, TWO_LEVEL>(*p, (uint64_t)sample * npix + px, L, sample == 0 ? it->primary : nullptr);
             sum[0] = fadd(sum[0], L[0]);
             sum[1] = fadd(sum[1], L[1]);
             sum[2] = fadd(sum[2], L[2]);
@@ -97,13 +97,13 @@ __global__ void __launch_bounds__(256) batch_kernel(const BatchItem* __restrict_
 }
 
 namespace {
-template <int CAP>
+template <int CAP, bool TWO_LEVEL>
 cudaError_t launch_cap(const BatchItem* items, uint32_t n_items, uint64_t first, uint64_t count, unsigned long long* counter,
                        const pt_batch_tuning& t, unsigned long long* rays, cudaStream_t s) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<CAP>, (int)t.threads_per_block, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel<CAP, TWO_LEVEL>, (int)t.threads_per_block, 0);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     const uint64_t warps_needed = (count + t.queue_chunk - 1) / t.queue_chunk;
@@ -112,7 +112,8 @@ cudaError_t launch_cap(const BatchItem* items, uint32_t n_items, uint64_t first,
     if (grid > grid_needed) grid = grid_needed ? grid_needed : 1;
     e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
-    batch_kernel<CAP><<<(unsigned)grid, t.threads_per_block, 0, s>>>(items, n_items, first, count, counter, t.queue_chunk, rays);
+    batch_kernel<CAP, TWO_LEVEL><<<(unsigned)grid, t.threads_per_block, 0, s>>>(items, n_items, first, count, counter,
+                                                                              t.queue_chunk, rays);
     return cudaGetLastError();
 }
 }  // namespace
@@ -126,13 +127,21 @@ int stack_cap_for(uint32_t max_tree_depth, uint32_t requested) {
 }
 
 cudaError_t launch_batch(const BatchItem* items, uint32_t n_items, uint64_t first, uint64_t count, unsigned long long* counter,
-                         const pt_batch_tuning& t, int cap, unsigned long long* rays, cudaStream_t s) {
+                         const pt_batch_tuning& t, int cap, unsigned long long* rays, cudaStream_t s, bool two_level) {
     if (count == 0) return cudaSuccess;
+    if (two_level) {  // some item is a two-level scene: the kernel that handles both layouts
+        switch (cap) {
+            case 24: return launch_cap<24, true>(items, n_items, first, count, counter, t, rays, s);
+            case 32: return launch_cap<32, true>(items, n_items, first, count, counter, t, rays, s);
+            case 48: return launch_cap<48, true>(items, n_items, first, count, counter, t, rays, s);
+            default: return launch_cap<64, true>(items, n_items, first, count, counter, t, rays, s);
+        }
+    }
     switch (cap) {
-        case 24: return launch_cap<24>(items, n_items, first, count, counter, t, rays, s);
-        case 32: return launch_cap<32>(items, n_items, first, count, counter, t, rays, s);
-        case 48: return launch_cap<48>(items, n_items, first, count, counter, t, rays, s);
-        default: return launch_cap<64>(items, n_items, first, count, counter, t, rays, s);
+        case 24: return launch_cap<24, false>(items, n_items, first, count, counter, t, rays, s);
+        case 32: return launch_cap<32, false>(items, n_items, first, count, counter, t, rays, s);
+        case 48: return launch_cap<48, false>(items, n_items, first, count, counter, t, rays, s);
+        default: return launch_cap<64, false>(items, n_items, first, count, counter, t, rays, s);
     }
 }
 
@@ -159,6 +168,7 @@ struct pt_batch {
     pt_batch_tuning tuning{};
     int cap = 64;
     int device = 0;
+    bool two_level = false;   // some item is a two-level scene (fused pipeline only)
     void* params = nullptr;   // RenderParams[n]
     void* items = nullptr;    // BatchItem[n]
     void* films = nullptr;    // all rgb outputs
@@ -278,6 +288,11 @@ extern "C" int pt_batch_create(const pt_batch_item* items, uint32_t n, const pt_
         if (items[i].desc.flags & (PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT | PT_RENDER_FUSED))
             return fail(PT_EINVAL, "batch items take the batch's pipeline (no PT_RENDER_WAVEFRONT / PERSISTENT / FUSED)");
         if (i && items[i].scene->device != items[0].scene->device) return fail(PT_EINVAL, "batch items on different devices");
+        if (items[i].scene->two_level) {
+            if (t.pipeline != PT_PIPELINE_FUSED)
+                return fail(PT_EINVAL, "batch item " + std::to_string(i) + ": a two-level scene needs PT_PIPELINE_FUSED");
+            b->two_level = true;
+        }
         max_depth = std::max(max_depth, items[i].scene->max_depth);
         b->scenes.push_back(items[i].scene);
         hp[i] = render_params(items[i].scene, &items[i].desc);
@@ -330,7 +345,7 @@ extern "C" int pt_batch_create(const pt_batch_item* items, uint32_t n, const pt_
         const uint64_t wave = t.wave_pixels ? t.wave_pixels : b->total_pixels;
         for (uint64_t first = 0; e == cudaSuccess && first < b->total_pixels; first += wave) {
             const uint64_t cnt = std::min<uint64_t>(wave, b->total_pixels - first);
-            e = launch_batch((const BatchItem*)b->items, n, first, cnt, ctr, t, b->cap, ctr + 1, b->stream);
+            e = launch_batch((const BatchItem*)b->items, n, first, cnt, ctr, t, b->cap, ctr + 1, b->stream, b->two_level);
         }
     } else if (e == cudaSuccess) {
         e = wf_enqueue(b.get(), ctr + 1);

@@ -24,8 +24,9 @@ struct BatchItem {
 // Smallest supported stack capacity >= max(tree depth + 2, requested); 0 if none fits.
 int stack_cap_for(uint32_t max_tree_depth, uint32_t requested);
 int check_tuning(const pt_batch_tuning& t);
+// two_level: some item is a two-level scene (the kernel then handles both layouts).
 cudaError_t launch_batch(const BatchItem* items, uint32_t n_items, uint64_t first, uint64_t count,
                          unsigned long long* counter, const pt_batch_tuning& t, int cap, unsigned long long* rays,
-                         cudaStream_t s);
+                         cudaStream_t s, bool two_level = false);
 
 }  // namespace pt

@@ -4,6 +4,8 @@
 // Traversal stack entries per ray.  The reference's ordered DFS needs at most (tree depth + 1)
 // entries; pt_scene_create records the depth and calls refuse trees that do not fit.
 #define PT_TRAVERSAL_STACK 64
+// Top-level stack entries of a two-level scene (pt_scene_create_two_level refuses deeper trees).
+#define PT_TOP_STACK 64
 
 // Warp rounds of the persistent walks (walk_round, traverse.cuh): the lanes of a warp take node
 // steps together until this many of them hold a leaf or have ended their walk (32 = every walking

@@ -20,6 +20,10 @@ struct TraceArgs {
     void* counter;         // device 64-bit ray counter for the persistent kernel (null: one thread per ray)
     int shared_stack;      // stack entries per lane kept in shared memory (0, 8 or 16)
     uint32_t chunk;        // rays a warp takes per fetch (0 = 64)
+    // two-level scenes: instances and the top-level tree (null for a flattened scene)
+    const void* instances = nullptr;
+    const void* top_nodes = nullptr;
+    uint32_t top_num_nodes = 0;
 };
 
 cudaError_t launch_trace(const TraceArgs& a, cudaStream_t s);

@@ -6,6 +6,7 @@
 #pragma once
 
 #include "shade.cuh"
+#include "two_level.cuh"
 
 namespace pt {
 
@@ -29,19 +30,12 @@ PT_HD bool throughput_is_zero(const F3& s) {  // ReflectanceSpectrum::is_zero
 }
 
 // One loop iteration of PathTraceIntegrator::GetSample after the intersection (lines 46-132 of
-// PathTraceIntegrator.cpp, patched as described in shade.cuh).  Returns true when the path goes on
-// with the new ray in s.o / s.d; fills `sh` when a shadow ray must be traced.
-PT_HD bool shade_hit(const RenderParams& p, PathState& s, uint32_t prim, uint32_t leaf, float u,
-                                          float v, float w, uint32_t pixel, uint32_t sample, ShadowReq& sh) {
-    sh.valid = false;
+// PathTraceIntegrator.cpp, patched as described in shade.cuh), given the hit face's world vertices
+// and mesh.  Returns true when the path goes on with the new ray in s.o / s.d; fills `sh` when a
+// shadow ray must be traced.
+PT_HD bool shade_face(const RenderParams& p, PathState& s, uint32_t prim, F3 v0, F3 v1, F3 v2, uint32_t mesh,
+                      float u, float v, float w, uint32_t pixel, uint32_t sample, ShadowReq& sh) {
     const bool nee = (p.flags & PT_RENDER_NEE) && p.num_lights > 0;
-    if (prim == kPrimNone) {
-        if (p.has_env) s.L = vadd(s.L, f3(fmul(p.env[0], s.src.x), fmul(p.env[1], s.src.y), fmul(p.env[2], s.src.z)));
-        return false;
-    }
-    F3 v0, v1, v2;
-    uint32_t mesh;
-    load_face((const float4*)p.tris, leaf, v0, v1, v2, mesh);
     const MeshRec mr = ((const MeshRec*)p.meshes)[mesh];
     if (mr.is_light) {
         if (!(nee && s.last_lambert))
@@ -93,6 +87,46 @@ PT_HD bool shade_hit(const RenderParams& p, PathState& s, uint32_t prim, uint32_
     return true;
 }
 
+PT_HD bool shade_miss(const RenderParams& p, PathState& s) {
+    if (p.has_env) s.L = vadd(s.L, f3(fmul(p.env[0], s.src.x), fmul(p.env[1], s.src.y), fmul(p.env[2], s.src.z)));
+    return false;
+}
+
+// The shading step of a flattened scene: the hit face's world vertices from the leaf-ordered
+// face records.
+PT_HD bool shade_hit(const RenderParams& p, PathState& s, uint32_t prim, uint32_t leaf, float u,
+                                          float v, float w, uint32_t pixel, uint32_t sample, ShadowReq& sh) {
+    sh.valid = false;
+    if (prim == kPrimNone) return shade_miss(p, s);
+    F3 v0, v1, v2;
+    uint32_t mesh;
+    load_face((const float4*)p.tris, leaf, v0, v1, v2, mesh);
+    return shade_face(p, s, prim, v0, v1, v2, mesh, u, v, w, pixel, sample, sh);
+}
+
+// The shading step of a two-level scene: the object-space face record carried to world space
+// with its instance's object_to_world, as the flattened scene's vertices were baked.
+PT_HD bool shade_hit_two_level(const RenderParams& p, PathState& s, uint32_t prim, uint32_t face, uint32_t inst,
+                               float u, float v, float w, uint32_t pixel, uint32_t sample, ShadowReq& sh) {
+    sh.valid = false;
+    if (prim == kPrimNone) return shade_miss(p, s);
+    const float4* tris = (const float4*)p.tris;
+    const float4 q0 = ldg(tris + 3 * (size_t)face), q1 = ldg(tris + 3 * (size_t)face + 1), q2 = ldg(tris + 3 * (size_t)face + 2);
+    const DeviceInstance* in = (const DeviceInstance*)p.instances + inst;
+    float m[16];
+    for (int k = 0; k < 16; ++k) m[k] = ldg(in->o2w + k);
+    F3 v0 = f3(q0.x, q0.y, q0.z), v1 = f3(q0.w, q1.x, q1.y), v2 = f3(q1.z, q1.w, q2.x);
+    apply_point_dev(m, v0.x, v0.y, v0.z);
+    apply_point_dev(m, v1.x, v1.y, v1.z);
+    apply_point_dev(m, v2.x, v2.y, v2.z);
+    return shade_face(p, s, prim, v0, v1, v2, ldg(&in->mesh), u, v, w, pixel, sample, sh);
+}
+
+PT_HD TwoLevelView two_level_view(const RenderParams& p) {
+    return TwoLevelView{(const uint4*)p.nodes, (const float4*)p.tris, p.num_nodes, (const uint4*)p.top_nodes,
+                        p.top_num_nodes, (const DeviceInstance*)p.instances};
+}
+
 // Camera ray of a path (pixel centre, or jittered with the (pixel, sample, 0xFFFF) RNG block).
 PT_HD void path_camera(const RenderParams& p, uint64_t path, uint32_t& pixel, uint32_t& sample,
                                             F3& o, F3& d) {
@@ -118,9 +152,44 @@ PT_HD void clamp_store(float* out, const F3& L) {  // BoxFilter::AddSample clamp
 
 // ---- fused pipeline -------------------------------------------------------------------------
 
-// Returns the number of rays traced (camera + bounce + shadow).
-template <int CAP = kStackCap>
+// The fused path loop on a two-level scene (same steps as path_fused).
+template <int CAP>
+PT_HD uint32_t path_fused_two_level(const RenderParams& p, uint64_t path, float* out, uint32_t* primary) {
+    const TwoLevelView view = two_level_view(p);
+    const float inf = bitsf(0x7F800000u);
+    uint32_t pixel, sample;
+    PathState s;
+    path_camera(p, path, pixel, sample, s.o, s.d);
+    s.src = f3(1.f, 1.f, 1.f);
+    s.L = f3(0.f, 0.f, 0.f);
+    s.bounces = 0;
+    s.last_lambert = 0;
+    uint32_t rays = 0;
+    while (!throughput_is_zero(s.src)) {
+        const TwoLevelHit h = traverse_two_level<false, CAP>(view, s.o.x, s.o.y, s.o.z, s.d.x, s.d.y, s.d.z, inf, false);
+        ++rays;
+        if (h.r.overflow) { raise_flag(p.err); break; }
+        if (s.bounces == 0 && sample == 0 && primary) primary[pixel] = h.r.prim;
+        ShadowReq sh;
+        const bool more = shade_hit_two_level(p, s, h.r.prim, h.r.leaf, h.inst, h.r.u, h.r.v, h.r.w, pixel, sample, sh);
+        if (sh.valid) {
+            const TwoLevelHit t = traverse_two_level<false, CAP>(view, sh.o.x, sh.o.y, sh.o.z, sh.wi.x, sh.wi.y, sh.wi.z,
+                                                                 sh.tmax, true);
+            ++rays;
+            if (t.r.overflow) { raise_flag(p.err); break; }
+            if (t.r.prim == kPrimNone) s.L = vadd(s.L, sh.contrib);
+        }
+        if (!more) break;
+    }
+    clamp_store(out, s.L);
+    return rays;
+}
+
+// Returns the number of rays traced (camera + bounce + shadow).  TWO_LEVEL: the scene may be a
+// two-level one (p.instances), traced with traverse_two_level.
+template <int CAP = kStackCap, bool TWO_LEVEL = false>
 PT_HD uint32_t path_fused(const RenderParams& p, uint64_t path, float* out, uint32_t* primary) {
+    if (TWO_LEVEL && p.instances) return path_fused_two_level<CAP>(p, path, out, primary);
     const uint4* nodes = (const uint4*)p.nodes;
     const float4* tris = (const float4*)p.tris;
     const float inf = bitsf(0x7F800000u);

@@ -12,6 +12,7 @@
 
 #include "../../include/polytope_b200.h"
 #include "config.h"
+#include "instance.h"
 
 #define PT_RAY_COUNTERS 256
 
@@ -86,8 +87,21 @@ struct HostScene {  // host copy of everything a scene handle uploads
     uint32_t num_prims = 0;
     uint32_t max_depth = 0;
     std::vector<uint32_t> prim_base;
+    // two-level layout (pt_scene_create_two_level): `nodes` / `tris` then hold every distinct
+    // geometry's object-space tree and faces back to back, and these the instances and the top
+    // level over their world boxes
+    bool two_level = false;
+    std::vector<DeviceInstance> instances;
+    std::vector<pt_bvh_node> tlas;
+    uint32_t tlas_depth = 0;
+    uint32_t num_geometries = 0;
 };
 int prepare_scene_host(const pt_scene_desc* desc, HostScene& out);
+// The two-level layout of a scene description (tlas.cpp); shading data as prepare_scene_host.
+int prepare_two_level_host(const pt_scene_desc* desc, HostScene& out);
+// Shading records, world vertex normals and the area-light table of a scene (abi.cpp), shared by
+// both layouts.
+void prepare_shading_host(const pt_scene_desc* desc, const WorldMeshes& w, HostScene& h);
 
 struct SceneDev {
     // traversal data
@@ -101,6 +115,11 @@ struct SceneDev {
     void* light_cdf = nullptr;    // num_lights floats
     uint32_t num_lights = 0;
     float light_area = 0.f;
+    // two-level scenes only
+    void* instances = nullptr;    // num_instances * DeviceInstance, in top-level leaf order
+    void* tlas_nodes = nullptr;   // tlas_num_nodes * 32 B
+    uint32_t num_instances = 0;
+    uint32_t tlas_num_nodes = 0;
 };
 
 }  // namespace pt
@@ -131,6 +150,7 @@ struct pt_scene {
     // that holds staging_mu
     void* err_flag = nullptr;
     void* trace_err = nullptr;
+    bool two_level = false;  // made by pt_scene_create_two_level
     // ray counters of the persistent trace kernel: one per launch in flight, taken round-robin
     void* ray_counters = nullptr;
     std::atomic<uint32_t> counter_next{0};

@@ -27,11 +27,12 @@ static_assert(sizeof(pt::MeshRec) == sizeof(pt::DeviceMesh) && alignof(pt::MeshR
 
 namespace pt {
 
+template <bool TWO_LEVEL>
 __global__ void __launch_bounds__(128) path_kernel(const RenderParams p, uint64_t first, uint32_t count,
                                                    float* __restrict__ radiance, uint32_t* __restrict__ primary) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     uint32_t rays = 0;
-    if (i < count) rays = path_fused(p, first + i, radiance + 3 * (size_t)i, primary);
+    if (i < count) rays = path_fused<kStackCap, TWO_LEVEL>(p, first + i, radiance + 3 * (size_t)i, primary);
     if (p.rays_traced) {
         const uint32_t sum = __reduce_add_sync(0xFFFFFFFFu, rays);
         if ((threadIdx.x & 31u) == 0 && sum) atomicAdd(p.rays_traced, (unsigned long long)sum);
@@ -99,7 +100,10 @@ cudaError_t upload_async(void* dst, const void* src, size_t bytes, cudaStream_t 
 cudaError_t launch_path_wave(const RenderParams& p, uint64_t first, uint32_t count, float* radiance, uint32_t* primary,
                              cudaStream_t s) {
     if (!count) return cudaSuccess;
-    path_kernel<<<(count + 127) / 128, 128, 0, s>>>(p, first, count, radiance, primary);
+    if (p.instances)
+        path_kernel<true><<<(count + 127) / 128, 128, 0, s>>>(p, first, count, radiance, primary);
+    else
+        path_kernel<false><<<(count + 127) / 128, 128, 0, s>>>(p, first, count, radiance, primary);
     return cudaGetLastError();
 }
 
@@ -189,6 +193,9 @@ RenderParams render_params(const pt_scene* s, const pt_render_desc* desc) {
     p.seed_hi = (uint32_t)(desc->seed >> 32);
     p.flags = desc->flags;
     p.err = (int*)s->err_flag;
+    p.instances = s->dev.instances;
+    p.top_nodes = s->dev.tlas_nodes;
+    p.top_num_nodes = s->dev.tlas_num_nodes;
     return p;
 }
 
@@ -204,6 +211,9 @@ int check_render_desc(const pt_scene* s, const pt_render_desc* desc) {
     if (pipes & (pipes - 1))
         return fail(PT_EINVAL, "PT_RENDER_WAVEFRONT, PT_RENDER_PERSISTENT and PT_RENDER_FUSED exclude each other");
     if ((int)s->max_depth + 2 > PT_TRAVERSAL_STACK) return fail(PT_ESTACK, "tree too deep for the traversal stack");
+    if (s->two_level && (desc->flags & (PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT)))
+        return fail(PT_EINVAL, "a two-level scene renders with the fused pipeline (PT_RENDER_WAVEFRONT and "
+                               "PT_RENDER_PERSISTENT walk flattened trees only)");
     return PT_OK;
 }
 }  // namespace pt
@@ -220,7 +230,7 @@ int enqueue_frame(pt_scene* s, const pt_render_desc* desc, float* rgb_d, uint32_
     p.err = err;
     // Pipelines: the persistent path kernel unless PT_RENDER_FUSED or PT_RENDER_WAVEFRONT is given
     // (the wave engine runs both the queue-based kernels and the persistent path kernel).
-    const bool fused = (desc->flags & PT_RENDER_FUSED) != 0;
+    const bool fused = (desc->flags & PT_RENDER_FUSED) != 0 || s->two_level;
     const bool persistent = !fused && (desc->flags & PT_RENDER_WAVEFRONT) == 0;
     const bool wavefront = !fused;
     const uint64_t total = npix64 * desc->spp;

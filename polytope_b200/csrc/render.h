@@ -36,6 +36,11 @@ struct RenderParams {
     uint32_t flags;
     int* err;
     unsigned long long* rays_traced;  // optional: counts camera + bounce + shadow rays
+    // two-level scenes (pt_scene_create_two_level): instances (DeviceInstance, top-level leaf
+    // order) and the top-level tree; null for a flattened scene, whose nodes / tris are world space
+    const void* instances;
+    const void* top_nodes;
+    uint32_t top_num_nodes;
 };
 
 // Paths [first, first + count) in sample-major order (path p = sample * W*H + pixel).

@@ -287,9 +287,11 @@ cudaError_t pt_server::enqueue(WaveInFlight& w, const std::vector<uint32_t>& tak
         // wave's kernel, its last reader.
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(d_items, hi, sizeof(pt::BatchItem) * w.members.size(), cudaMemcpyHostToDevice, stream);
+        bool two_level = false;
+        for (Request* r : w.members) two_level = two_level || r->scene->two_level;
         if (e == cudaSuccess)
             e = pt::launch_batch((const pt::BatchItem*)d_items, (uint32_t)w.members.size(), 0, base,
-                                 (unsigned long long*)d_counters, cfg.tuning, cap, rays, stream);
+                                 (unsigned long long*)d_counters, cfg.tuning, cap, rays, stream, two_level);
     } else {
         // one segment of consecutive paths per request; tables through this slot's pinned staging
         pt::WfPlan plan;
@@ -572,6 +574,8 @@ extern "C" int pt_server_submit(pt_server* s, pt_scene* scene, const pt_render_d
     if (desc->flags & (PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT | PT_RENDER_FUSED))
         return fail(PT_EINVAL, "served requests take the server's pipeline (no PT_RENDER_WAVEFRONT / PERSISTENT / FUSED)");
     if (scene->device != s->device) return fail(PT_EINVAL, "scene lives on another device");
+    if (scene->two_level && s->wave_engine)
+        return fail(PT_EINVAL, "a two-level scene is served by the fused pipeline only (PT_PIPELINE_FUSED)");
     if (!stack_cap_for(scene->max_depth, s->cfg.tuning.stack_depth)) return fail(PT_ESTACK, "tree too deep");
     std::unique_ptr<Request> r(new Request());
     r->scene = scene;

@@ -6,6 +6,7 @@
 
 #include "launch.h"
 #include "traverse.cuh"
+#include "two_level.cuh"
 
 namespace pt {
 
@@ -140,8 +141,48 @@ __global__ void __launch_bounds__(128, 8) trace_persistent_kernel(const uint4* _
     }
 }
 
+// Ray queries on a two-level scene: one thread per ray, traverse_two_level.
+template <bool COUNT>
+__global__ void __launch_bounds__(128) trace_two_level_kernel(const TwoLevelView v, const float4* __restrict__ rays,
+                                                              uint4* __restrict__ hits, uint64_t n, uint32_t* node_tests,
+                                                              uint32_t* tri_tests, int* err) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 r0 = ld_stream(rays + 2 * i);
+    const float4 r1 = ld_stream(rays + 2 * i + 1);
+    const bool any = (__float_as_uint(r1.w) & 1u) != 0;
+    const TwoLevelHit th = traverse_two_level<COUNT>(v, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, r0.w, any);
+    uint4 h;
+    h.x = th.r.prim;
+    h.y = __float_as_uint(th.r.t);
+    h.z = __float_as_uint(th.r.u);
+    h.w = __float_as_uint(th.r.v);
+    if (th.r.overflow) {
+        h.x = 0xFFFFFFFEu;
+        atomicExch(err, 1);
+    }
+    st_stream(hits + i, h);
+    if (COUNT) {
+        if (node_tests) node_tests[i] = th.r.nodes;
+        if (tri_tests) tri_tests[i] = th.r.tris;
+    }
+}
+
 cudaError_t launch_trace(const TraceArgs& a, cudaStream_t s) {
     if (a.n == 0) return cudaSuccess;
+    if (a.instances) {
+        const TwoLevelView v{(const uint4*)a.nodes, (const float4*)a.tris, a.num_nodes, (const uint4*)a.top_nodes,
+                             a.top_num_nodes, (const DeviceInstance*)a.instances};
+        const uint64_t grid = (a.n + 127) / 128;
+        if (grid > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+        if (a.node_tests || a.tri_tests)
+            trace_two_level_kernel<true><<<(unsigned)grid, 128, 0, s>>>(v, (const float4*)a.rays, (uint4*)a.hits, a.n,
+                                                                        a.node_tests, a.tri_tests, a.err);
+        else
+            trace_two_level_kernel<false><<<(unsigned)grid, 128, 0, s>>>(v, (const float4*)a.rays, (uint4*)a.hits, a.n,
+                                                                         nullptr, nullptr, a.err);
+        return cudaGetLastError();
+    }
     if (a.counter) {
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
