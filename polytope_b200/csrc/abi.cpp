@@ -128,6 +128,7 @@ int scene_trace(pt_scene* s, const pt_ray* rays, uint64_t n, pt_hit* hits, uint3
     a.instances = s->dev.instances;
     a.top_nodes = s->dev.tlas_nodes;
     a.top_num_nodes = s->dev.tlas_num_nodes;
+    a.exact_tree = s->nan_boxes;
     auto next_counter = [s]() {
         return (void*)((unsigned long long*)s->ray_counters + (s->counter_next.fetch_add(1) % PT_RAY_COUNTERS));
     };
@@ -394,6 +395,13 @@ int create_from_host(const pt_scene_desc* desc, HostScene& h, pt_scene** out) {
     if (cudaMalloc(&s->err_flag, sizeof(int)) != cudaSuccess) { free_scene(s.release()); return fail(PT_ENOMEM, "cudaMalloc error flag"); }
     cudaMemset(s->err_flag, 0, sizeof(int));
     if (cudaMalloc(&s->ray_counters, 8 * PT_RAY_COUNTERS) != cudaSuccess) { free_scene(s.release()); return fail(PT_ENOMEM, "cudaMalloc ray counters"); }
+    auto has_nan = [](const std::vector<pt_bvh_node>& nodes) {
+        for (const pt_bvh_node& n : nodes)
+            for (int k = 0; k < 3; ++k)
+                if (n.bb_min[k] != n.bb_min[k] || n.bb_max[k] != n.bb_max[k]) return true;
+        return false;
+    };
+    s->nan_boxes = has_nan(h.nodes) || has_nan(h.tlas);
     if (h.two_level) {
         s->two_level = true;
         s->dev.num_instances = (uint32_t)h.instances.size();

@@ -24,6 +24,7 @@ struct TraceArgs {
     const void* instances = nullptr;
     const void* top_nodes = nullptr;
     uint32_t top_num_nodes = 0;
+    bool exact_tree = false;  // some box holds a NaN: every ray takes the exact box test
 };
 
 cudaError_t launch_trace(const TraceArgs& a, cudaStream_t s);

@@ -124,7 +124,7 @@ PT_HD bool shade_hit_two_level(const RenderParams& p, PathState& s, uint32_t pri
 
 PT_HD TwoLevelView two_level_view(const RenderParams& p) {
     return TwoLevelView{(const uint4*)p.nodes, (const float4*)p.tris, p.num_nodes, (const uint4*)p.top_nodes,
-                        p.top_num_nodes, (const DeviceInstance*)p.instances};
+                        p.top_num_nodes, (const DeviceInstance*)p.instances, p.exact_tree != 0};
 }
 
 // Camera ray of a path (pixel centre, or jittered with the (pixel, sample, 0xFFFF) RNG block).
@@ -204,7 +204,7 @@ PT_HD uint32_t path_fused(const RenderParams& p, uint64_t path, float* out, uint
     while (!throughput_is_zero(s.src)) {
         RayState rs;
         ray_setup(rs, s.o.x, s.o.y, s.o.z, s.d.x, s.d.y, s.d.z);
-        const TraceResult h = traverse<false, CAP>(nodes, tris, p.num_nodes, rs, inf, false);
+        const TraceResult h = traverse<false, CAP>(nodes, tris, p.num_nodes, rs, inf, false, p.exact_tree != 0);
         ++rays;
         if (h.overflow) { raise_flag(p.err); break; }
         if (s.bounces == 0 && sample == 0 && primary) primary[pixel] = h.prim;
@@ -213,7 +213,7 @@ PT_HD uint32_t path_fused(const RenderParams& p, uint64_t path, float* out, uint
         if (sh.valid) {
             RayState sr;
             ray_setup(sr, sh.o.x, sh.o.y, sh.o.z, sh.wi.x, sh.wi.y, sh.wi.z);
-            const TraceResult t = traverse<false, CAP>(nodes, tris, p.num_nodes, sr, sh.tmax, true);
+            const TraceResult t = traverse<false, CAP>(nodes, tris, p.num_nodes, sr, sh.tmax, true, p.exact_tree != 0);
             ++rays;
             if (t.overflow) { raise_flag(p.err); break; }
             if (t.prim == kPrimNone) s.L = vadd(s.L, sh.contrib);

@@ -151,6 +151,7 @@ struct pt_scene {
     void* err_flag = nullptr;
     void* trace_err = nullptr;
     bool two_level = false;  // made by pt_scene_create_two_level
+    bool nan_boxes = false;  // some tree box holds a NaN (every ray then takes the exact box test)
     // ray counters of the persistent trace kernel: one per launch in flight, taken round-robin
     void* ray_counters = nullptr;
     std::atomic<uint32_t> counter_next{0};

@@ -196,6 +196,7 @@ RenderParams render_params(const pt_scene* s, const pt_render_desc* desc) {
     p.instances = s->dev.instances;
     p.top_nodes = s->dev.tlas_nodes;
     p.top_num_nodes = s->dev.tlas_num_nodes;
+    p.exact_tree = s->nan_boxes ? 1u : 0u;
     return p;
 }
 

@@ -41,6 +41,7 @@ struct RenderParams {
     const void* instances;
     const void* top_nodes;
     uint32_t top_num_nodes;
+    uint32_t exact_tree;  // some tree box holds a NaN: every ray takes the exact box test
 };
 
 // Paths [first, first + count) in sample-major order (path p = sample * W*H + pixel).

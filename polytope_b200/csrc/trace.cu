@@ -14,7 +14,7 @@ template <bool COUNT>
 __global__ void __launch_bounds__(128) trace_kernel(const uint4* __restrict__ nodes, const float4* __restrict__ tris,
                                                     uint32_t num_nodes, const float4* __restrict__ rays,
                                                     uint4* __restrict__ hits, uint64_t n, uint32_t* node_tests,
-                                                    uint32_t* tri_tests, int* err) {
+                                                    uint32_t* tri_tests, int* err, bool exact_tree) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 r0 = ld_stream(rays + 2 * i);
@@ -22,7 +22,7 @@ __global__ void __launch_bounds__(128) trace_kernel(const uint4* __restrict__ no
     RayState rs;
     ray_setup(rs, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
     const bool any = (__float_as_uint(r1.w) & 1u) != 0;
-    const TraceResult tr = traverse<COUNT>(nodes, tris, num_nodes, rs, r0.w, any);
+    const TraceResult tr = traverse<COUNT>(nodes, tris, num_nodes, rs, r0.w, any, exact_tree);
     uint4 h;
     h.x = tr.prim;
     h.y = __float_as_uint(tr.t);
@@ -52,7 +52,8 @@ __global__ void __launch_bounds__(128, 8) trace_persistent_kernel(const uint4* _
                                                                const float4* __restrict__ tris, uint32_t num_nodes,
                                                                const float4* __restrict__ rays, uint4* __restrict__ hits,
                                                                uint64_t n, uint32_t* node_tests, uint32_t* tri_tests,
-                                                               int* err, unsigned long long* counter, uint32_t kChunk) {
+                                                               int* err, unsigned long long* counter, uint32_t kChunk,
+                                                               bool exact_tree) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t lt_mask = (1u << lane) - 1u;
     uint64_t pool_next = 0, pool_end = 0;
@@ -83,7 +84,7 @@ __global__ void __launch_bounds__(128, 8) trace_persistent_kernel(const uint4* _
                 idx = pool_next + rank;
                 const float4 r0 = ld_stream(rays + 2 * idx);
                 const float4 r1 = ld_stream(rays + 2 * idx + 1);
-                walk_begin(k, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, r0.w, (__float_as_uint(r1.w) & 1u) != 0);
+                walk_begin(k, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z, r0.w, (__float_as_uint(r1.w) & 1u) != 0, exact_tree);
                 active = true;
             }
             const uint64_t took = (uint64_t)__popc(need) < avail ? (uint64_t)__popc(need) : avail;
@@ -172,7 +173,7 @@ cudaError_t launch_trace(const TraceArgs& a, cudaStream_t s) {
     if (a.n == 0) return cudaSuccess;
     if (a.instances) {
         const TwoLevelView v{(const uint4*)a.nodes, (const float4*)a.tris, a.num_nodes, (const uint4*)a.top_nodes,
-                             a.top_num_nodes, (const DeviceInstance*)a.instances};
+                             a.top_num_nodes, (const DeviceInstance*)a.instances, a.exact_tree};
         const uint64_t grid = (a.n + 127) / 128;
         if (grid > 0x7FFFFFFFull) return cudaErrorInvalidValue;
         if (a.node_tests || a.tri_tests)
@@ -208,11 +209,11 @@ cudaError_t launch_trace(const TraceArgs& a, cudaStream_t s) {
         if (counted)
             kern_t<<<(unsigned)grid, 128, 0, s>>>((const uint4*)a.nodes, (const float4*)a.tris, a.num_nodes,
                                                   (const float4*)a.rays, (uint4*)a.hits, a.n, a.node_tests, a.tri_tests,
-                                                  a.err, (unsigned long long*)a.counter, a.chunk ? a.chunk : 64u);
+                                                  a.err, (unsigned long long*)a.counter, a.chunk ? a.chunk : 64u, a.exact_tree);
         else
             kern_f<<<(unsigned)grid, 128, 0, s>>>((const uint4*)a.nodes, (const float4*)a.tris, a.num_nodes,
                                                   (const float4*)a.rays, (uint4*)a.hits, a.n, nullptr, nullptr, a.err,
-                                                  (unsigned long long*)a.counter, a.chunk ? a.chunk : 64u);
+                                                  (unsigned long long*)a.counter, a.chunk ? a.chunk : 64u, a.exact_tree);
         return cudaGetLastError();
     }
     const uint32_t block = 128;
@@ -221,11 +222,11 @@ cudaError_t launch_trace(const TraceArgs& a, cudaStream_t s) {
     if (a.node_tests || a.tri_tests)
         trace_kernel<true><<<(unsigned)grid, block, 0, s>>>(
             (const uint4*)a.nodes, (const float4*)a.tris, a.num_nodes, (const float4*)a.rays, (uint4*)a.hits, a.n,
-            a.node_tests, a.tri_tests, a.err);
+            a.node_tests, a.tri_tests, a.err, a.exact_tree);
     else
         trace_kernel<false><<<(unsigned)grid, block, 0, s>>>(
             (const uint4*)a.nodes, (const float4*)a.tris, a.num_nodes, (const float4*)a.rays, (uint4*)a.hits, a.n,
-            nullptr, nullptr, a.err);
+            nullptr, nullptr, a.err, a.exact_tree);
     return cudaGetLastError();
 }
 
@@ -261,7 +262,11 @@ __global__ void selftest_box_kernel(const float* in, uint32_t* out, uint32_t n) 
     const float* c = in + 16 * (size_t)i;
     RayState r;
     ray_setup(r, c[6], c[7], c[8], c[9], c[10], c[11]);
-    out[i] = box_hits(r, c[0], c[1], c[2], c[3], c[4], c[5], c[12], needs_inside_test(r, c[12])) ? 1u : 0u;
+    // as a traversal runs it: the scene-level NaN flag set when this box holds a NaN, then the
+    // ray's own box mode (the min/max test for finite rays)
+    bool nan_box = false;
+    for (int k = 0; k < 6; ++k) nan_box = nan_box || c[k] != c[k];
+    out[i] = box_test(r, box_mode_for(r, c[12], nan_box), c[0], c[1], c[2], c[3], c[4], c[5], c[12]) ? 1u : 0u;
 }
 
 cudaError_t launch_selftest_box(const float* in16, uint32_t* hit, uint32_t n, cudaStream_t s) {

@@ -98,6 +98,40 @@ PT_HD bool box_hits(const RayState& r, float b0, float b1, float b2, float b3, f
     return near_t <= far_t;
 }
 
+// The same test for a ray whose origin and 1/d are finite and 1/d has no zero component, on a tree
+// whose boxes hold no NaN: then no (b - o) * (1/d) product is NaN (a NaN needs 0 * inf, inf - inf
+// or a NaN operand), and on non-NaN operands the reference's ternaries `a > b ? b : a` / `a > b ? a
+// : b` are min / max up to the sign of a zero, which the final `near <= far` comparison does not
+// see.  So one min / max instruction replaces each compare-and-select, and the inside early-out is
+// skipped as in box_hits (needs_inside_test is false for such rays when tmax >= 0).
+PT_HD bool box_hits_fast(const RayState& r, float b0, float b1, float b2, float b3, float b4, float b5, float min_t) {
+    const float gm = bitsf(PT_GAMMA_MUL_BITS);
+    const float x0 = fmul(fsub(b0, r.ox), r.ix), x1 = fmul(fsub(b3, r.ox), r.ix);
+    const float y0 = fmul(fsub(b1, r.oy), r.iy), y1 = fmul(fsub(b4, r.oy), r.iy);
+    const float z0 = fmul(fsub(b2, r.oz), r.iz), z1 = fmul(fsub(b5, r.oz), r.iz);
+    const float near_t = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), 0.f));
+    const float far_t = fminf(fminf(fmul(fmaxf(x0, x1), gm), fmul(fmaxf(y0, y1), gm)),
+                              fminf(fmul(fmaxf(z0, z1), gm), min_t));
+    return near_t <= far_t;
+}
+
+// Which box test a ray takes (walk state box_mode): 0 box_hits_fast, 1 box_hits without the inside
+// early-out, 2 box_hits with it.  `exact_tree`: the tree has a NaN in some box.
+PT_HD int box_mode_for(const RayState& r, float tmax, bool exact_tree) {
+    if (needs_inside_test(r, tmax)) return 2;
+    const float inf = bitsf(0x7F800000u);
+    const bool finite = fabs_(r.ox) < inf && fabs_(r.oy) < inf && fabs_(r.oz) < inf && fabs_(r.ix) < inf &&
+                        fabs_(r.iy) < inf && fabs_(r.iz) < inf && r.ix != 0.f && r.iy != 0.f && r.iz != 0.f;
+    return (finite && !exact_tree) ? 0 : 1;
+}
+
+// Measured on a B200 against box_hits for every ray (two runs each, same box): 1.3 M-face ray
+// queries 2150 vs 2104 Mrays/s, the 256-scene batch 2189 vs 1966 Mrays/s (wavefront pipeline) and
+// 1662 vs 1631 (path pipeline), the 6.5 M-face frame's fused kernel 954 vs 922 Msamples/s.
+PT_HD bool box_test(const RayState& r, int mode, float b0, float b1, float b2, float b3, float b4, float b5, float min_t) {
+    return mode == 0 ? box_hits_fast(r, b0, b1, b2, b3, b4, b5, min_t) : box_hits(r, b0, b1, b2, b3, b4, b5, min_t, mode == 2);
+}
+
 PT_HD float max3abs(float x, float y, float z) {  // max_component(abs(v)), mesh.cpp:145-155
     x = fabs_(x); y = fabs_(y); z = fabs_(z);
     if (x >= y && x >= z) return x;
@@ -190,16 +224,17 @@ struct RayWalkT {
     float u, v, w;
     uint32_t nodes, tris;
     bool any, done;
-    bool check_inside;  // needs_inside_test for this ray
+    int box_mode;       // box_mode_for this ray
     int sp;
     WalkStack<CAP, SH> stack;
 };
 using RayWalk = RayWalkT<>;
 
 template <int CAP, int SH>
-PT_HD void walk_begin(RayWalkT<CAP, SH>& k, float ox, float oy, float oz, float dx, float dy, float dz, float tmax, bool any) {
+PT_HD void walk_begin(RayWalkT<CAP, SH>& k, float ox, float oy, float oz, float dx, float dy, float dz, float tmax, bool any,
+                      bool exact_tree = false) {
     ray_setup(k.r, ox, oy, oz, dx, dy, dz);
-    k.check_inside = needs_inside_test(k.r, tmax);
+    k.box_mode = box_mode_for(k.r, tmax, exact_tree);
     k.min_t = tmax;
     k.prim = kPrimNone;
     k.leaf = kPrimNone;
@@ -223,7 +258,7 @@ PT_HD int walk_step(RayWalkT<CAP, SH>& k, const uint4* __restrict__ nodes, uint3
     uint4 a, b;
     ldg_node(nodes + 2 * (size_t)ni, a, b);
     if (COUNT) k.nodes++;
-    if (!box_hits(k.r, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), k.min_t, k.check_inside))
+    if (!box_test(k.r, k.box_mode, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), k.min_t))
         return 0;
     const uint32_t nf = b.w & 0xFFFFu;
     if (nf > 0) {
@@ -254,7 +289,7 @@ PT_HD bool walk_to_leaf(RayWalkT<CAP, SH>& k, const uint4* __restrict__ nodes, u
         uint4 a, b;
         ldg_node(nodes + 2 * (size_t)ni, a, b);
         if (COUNT) k.nodes++;
-        if (!box_hits(k.r, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), k.min_t, k.check_inside))
+        if (!box_test(k.r, k.box_mode, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), k.min_t))
             continue;
         const uint32_t nf = b.w & 0xFFFFu;
         if (nf > 0) {
@@ -339,7 +374,8 @@ struct TraceResult {
 // the stack capacity (tree depth + 2 must fit; the host checks before launching).
 template <bool COUNT, int CAP = kStackCap>
 PT_HD TraceResult traverse(const uint4* __restrict__ nodes, const float4* __restrict__ tris,
-                                                uint32_t num_nodes, const RayState& r, float tmax, bool any) {
+                                                uint32_t num_nodes, const RayState& r, float tmax, bool any,
+                                                bool exact_tree = false) {
     TraceResult res;
     res.prim = kPrimNone;
     res.leaf = kPrimNone;
@@ -348,7 +384,7 @@ PT_HD TraceResult traverse(const uint4* __restrict__ nodes, const float4* __rest
     res.nodes = res.tris = 0;
     res.overflow = false;
     const bool neg_x = r.ix < 0, neg_y = r.iy < 0, neg_z = r.iz < 0;
-    const bool check_inside = needs_inside_test(r, tmax);
+    const int box_mode = box_mode_for(r, tmax, exact_tree);
     uint32_t stack[CAP];
     int sp = 0;
     stack[sp++] = 0;
@@ -359,8 +395,7 @@ PT_HD TraceResult traverse(const uint4* __restrict__ nodes, const float4* __rest
         uint4 a, b;
         ldg_node(nodes + 2 * (size_t)ni, a, b);
         if (COUNT) res.nodes++;
-        if (!box_hits(r, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w),
-                      bitsf(b.x), bitsf(b.y), min_t, check_inside))
+        if (!box_test(r, box_mode, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), min_t))
             continue;
         const uint32_t nf = b.w & 0xFFFFu;
         if (nf > 0) {

@@ -23,6 +23,7 @@ struct TwoLevelView {
     const uint4* top;            // top-level nodes
     uint32_t top_nodes;
     const DeviceInstance* inst;  // instances in top-level leaf order
+    bool exact_tree;             // some box holds a NaN: every ray takes the exact box test
 };
 
 struct TwoLevelHit {
@@ -68,7 +69,7 @@ PT_HD TwoLevelHit traverse_two_level(const TwoLevelView& v, float ox, float oy, 
     RayState wr;
     ray_setup(wr, ox, oy, oz, dx, dy, dz);
     const bool wneg_x = wr.ix < 0, wneg_y = wr.iy < 0, wneg_z = wr.iz < 0;
-    const bool wcheck = needs_inside_test(wr, tmax);
+    const int wmode = box_mode_for(wr, tmax, v.exact_tree);
     float min_t = tmax;
     uint32_t tstack[kTopStackCap];
     int tsp = 0;
@@ -80,7 +81,7 @@ PT_HD TwoLevelHit traverse_two_level(const TwoLevelView& v, float ox, float oy, 
         uint4 a, b;
         ldg_node(v.top + 2 * (size_t)ti, a, b);
         if (COUNT) res.nodes++;
-        if (!box_hits(wr, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), min_t, wcheck)) continue;
+        if (!box_test(wr, wmode, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), min_t)) continue;
         const uint32_t nf = b.w & 0xFFFFu;
         if (nf == 0) {
             if (tsp + 2 > kTopStackCap) { res.overflow = true; return out; }
@@ -104,7 +105,7 @@ PT_HD TwoLevelHit traverse_two_level(const TwoLevelView& v, float ox, float oy, 
             RayState r;
             ray_setup(r, lox, loy, loz, ldx, ldy, ldz);
             const bool neg_x = r.ix < 0, neg_y = r.iy < 0, neg_z = r.iz < 0;
-            const bool check_inside = needs_inside_test(r, min_t);
+            const int mode = box_mode_for(r, min_t, v.exact_tree);
             int sp = 0;
             stack[sp++] = root;
             while (sp > 0) {
@@ -113,8 +114,7 @@ PT_HD TwoLevelHit traverse_two_level(const TwoLevelView& v, float ox, float oy, 
                 uint4 na, nb;
                 ldg_node(v.nodes + 2 * (size_t)ni, na, nb);
                 if (COUNT) res.nodes++;
-                if (!box_hits(r, bitsf(na.x), bitsf(na.y), bitsf(na.z), bitsf(na.w), bitsf(nb.x), bitsf(nb.y), min_t,
-                              check_inside))
+                if (!box_test(r, mode, bitsf(na.x), bitsf(na.y), bitsf(na.z), bitsf(na.w), bitsf(nb.x), bitsf(nb.y), min_t))
                     continue;
                 const uint32_t nfaces = nb.w & 0xFFFFu;
                 if (nfaces > 0) {

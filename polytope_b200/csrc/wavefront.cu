@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(256, kWfTraceMinBlocks) wf_trace_kernel(const 
                 tris = (const float4*)p->tris;
                 num_nodes = p->num_nodes;
                 err = p->err;
-                walk_begin(k, o4.x, o4.y, o4.z, d4.x, d4.y, d4.z, tmax, SHADOW);
+                walk_begin(k, o4.x, o4.y, o4.z, d4.x, d4.y, d4.z, tmax, SHADOW, p->exact_tree != 0);
                 active = true;
                 ++rays;
             }
@@ -249,7 +249,7 @@ enum ColdField : uint32_t {
     kOx, kOy, kOz, kDx, kDy, kDz, kSr, kSg, kSb, kLr, kLg, kLb, kCr, kCg, kCb,
     kBounces, kFlags, kSlot, kPixel, kSample, kItem, kColdFields
 };
-constexpr uint32_t kColdShadow = 1u, kColdPending = 2u, kColdLambert = 4u;
+constexpr uint32_t kColdShadow = 1u, kColdPending = 2u, kColdLambert = 4u, kColdExact = 8u;  // kColdExact: NaN boxes
 
 struct ColdLane {
     uint32_t* c;  // this lane's field 0
@@ -308,6 +308,7 @@ __global__ void __launch_bounds__(128, 8) wf_path_kernel(const WfItem* __restric
                 nodes = (const uint4*)p->nodes;
                 tris = (const float4*)p->tris;
                 num_nodes = p->num_nodes;
+                const bool exact = p->exact_tree != 0;
                 uint32_t pixel, sample;
                 F3 o, d;
                 path_camera(*p, sg.local_begin + (slot - sg.slot_base), pixel, sample, o, d);
@@ -316,12 +317,12 @@ __global__ void __launch_bounds__(128, 8) wf_path_kernel(const WfItem* __restric
                 cold.set3(kSr, f3(1.f, 1.f, 1.f));
                 cold.set3(kLr, f3(0.f, 0.f, 0.f));
                 cold.set(kBounces, 0u);
-                cold.set(kFlags, 0u);
+                cold.set(kFlags, exact ? kColdExact : 0u);
                 cold.set(kSlot, slot);
                 cold.set(kPixel, pixel);
                 cold.set(kSample, sample);
                 cold.set(kItem, item);
-                walk_begin(k, o.x, o.y, o.z, d.x, d.y, d.z, inf, false);
+                walk_begin(k, o.x, o.y, o.z, d.x, d.y, d.z, inf, false, exact);
                 active = true;
                 finished = false;
             }
@@ -359,6 +360,7 @@ __global__ void __launch_bounds__(128, 8) wf_path_kernel(const WfItem* __restric
                 const RenderParams* p = it.params;
                 uint32_t flags = cold.u(kFlags);
                 const bool shadow = (flags & kColdShadow) != 0;
+                const bool exact = (flags & kColdExact) != 0;
                 bool go = false, next_shadow = false;
                 if (!walk_ok) {
                     raise_flag(p->err);
@@ -379,12 +381,12 @@ __global__ void __launch_bounds__(128, 8) wf_path_kernel(const WfItem* __restric
                     cold.set3(kSr, s.src);
                     cold.set3(kLr, s.L);
                     cold.set(kBounces, s.bounces);
-                    flags = s.last_lambert ? kColdLambert : 0u;
+                    flags = (s.last_lambert ? kColdLambert : 0u) | (flags & kColdExact);
                     if (sh.valid) {
                         cold.set3(kCr, sh.contrib);
                         flags |= kColdShadow | (more ? kColdPending : 0u);
                         next_shadow = true;
-                        walk_begin(k, sh.o.x, sh.o.y, sh.o.z, sh.wi.x, sh.wi.y, sh.wi.z, sh.tmax, true);
+                        walk_begin(k, sh.o.x, sh.o.y, sh.o.z, sh.wi.x, sh.wi.y, sh.wi.z, sh.tmax, true, exact);
                     } else {
                         go = more && !throughput_is_zero(s.src);
                     }
@@ -397,7 +399,7 @@ __global__ void __launch_bounds__(128, 8) wf_path_kernel(const WfItem* __restric
                 if (!next_shadow) {
                     if (go) {
                         const F3 o = cold.f3at(kOx), d = cold.f3at(kDx);
-                        walk_begin(k, o.x, o.y, o.z, d.x, d.y, d.z, inf, false);
+                        walk_begin(k, o.x, o.y, o.z, d.x, d.y, d.z, inf, false, exact);
                     } else {
                         clamp_store(radiance + 3 * (size_t)cold.u(kSlot), cold.f3at(kLr));
                         active = false;
