@@ -35,6 +35,7 @@
 
 #include "batch.h"
 #include "pt_internal.h"
+#include "serve_sched.h"
 #include "wavefront.h"
 
 using Clock = std::chrono::steady_clock;
@@ -43,21 +44,19 @@ namespace {
 
 constexpr int kWavesQueued = 2;  // waves enqueued on the stream at once (host planning overlaps the GPU)
 
-struct Request {
+// A request; its scheduling state (state, cancel, total and planned work units -- pixels for the
+// fused pipeline, sample-major paths for the wave pipelines) is the serve::Work base.
+struct Request : pt::serve::Work {
     uint64_t ticket = 0;
     pt_scene* scene = nullptr;
     pt_render_desc desc{};
     pt::RenderParams params{};
     uint32_t npix = 0;
-    uint64_t total = 0;           // work units: pixels (fused) or paths (wave pipelines, sample-major)
-    uint64_t planned = 0;         // units handed to waves so far
     size_t bytes = 0;             // device bytes
     void* dev = nullptr;          // RenderParams, rgb (3 floats/px), primary ids, film sums (wave pipelines)
     size_t host_off = ~(size_t)0; // finished film in the host arena: rgb then primary ids
     uint32_t param_slot = ~0u;    // pinned staging slot of its parameters while admitted
-    int state = 0;                // 0 queued, 1 admitted, 2 done, 3 cancelled, < 0 error
     bool launched = false, retired = false;
-    bool cancel = false;          // pt_server_cancel while admitted: no more waves, then dropped
     uint32_t waves_queued = 0;    // queued waves that hold work of this request
     Clock::time_point submitted, admitted, first_wave, last_wave, done;
 };
@@ -177,7 +176,7 @@ struct pt_server {
     void finish_cancel(Request* r);   // with mu held
     bool has_unplanned() const {
         for (const Request* r : active)
-            if (r->state == 1 && !r->cancel && r->planned < r->total) return true;
+            if (pt::serve::open(*r)) return true;
         return false;
     }
 };
@@ -192,7 +191,7 @@ void pt_server::admit() {
     while (!pending.empty() && active.size() < cfg.max_inflight) {
         Request* r = pending.front();
         const size_t need = request_bytes(r->npix, wave_engine);
-        if (mem_in_use + need > budget && !active.empty()) {
+        if (!pt::serve::fits(mem_in_use, need, budget, active.empty())) {
             blocked = true;
             break;
         }
@@ -232,30 +231,22 @@ void pt_server::admit() {
     }
 }
 
-// Picks the next wave's work (mu held): oldest admitted request first, each taking what it has
-// left up to the wave's room, or an equal share of the wave for every request.
+// Picks the next wave's work (mu held) by the configured policy (serve::plan_wave).
 void pt_server::plan(WaveInFlight& w, std::vector<uint32_t>& take, std::vector<uint64_t>& first) {
-    uint64_t room = wave_engine ? std::min<uint64_t>(cfg.wave_pixels, ws.capacity) : cfg.wave_pixels;
-    uint64_t share = room;
-    if (cfg.policy == PT_SERVE_FAIR_SHARE) {
-        size_t open = 0;
-        for (const Request* r : active) open += r->state == 1 && r->planned < r->total;
-        if (open) share = std::max<uint64_t>(1024, room / open);
-    }
-    for (Request* r : active) {
-        if (w.members.size() >= max_items || room == 0) break;
-        if (r->state != 1 || r->cancel || r->planned >= r->total) continue;
-        const uint64_t t = std::min<uint64_t>(std::min<uint64_t>(share, r->total - r->planned), room);
-        room -= t;
+    const uint64_t room = wave_engine ? std::min<uint64_t>(cfg.wave_pixels, ws.capacity) : cfg.wave_pixels;
+    std::vector<pt::serve::Work*> view(active.begin(), active.end());
+    std::vector<pt::serve::Take> takes;
+    pt::serve::plan_wave(view, room, cfg.policy, max_items, takes);
+    for (const pt::serve::Take& t : takes) {
+        Request* r = active[t.index];
         if (!r->launched) {
             r->launched = true;
             r->first_wave = Clock::now();
         }
         w.members.push_back(r);
         ++r->waves_queued;
-        take.push_back((uint32_t)t);
-        first.push_back(r->planned);
-        r->planned += t;
+        take.push_back((uint32_t)t.count);
+        first.push_back(t.first);
         if (r->planned == r->total) w.finishing.push_back(r);
     }
 }
@@ -413,7 +404,7 @@ void pt_server::retire(WaveInFlight& w) {
             }
             // cancelled requests whose last queued wave this was
             for (Request* r : w.members)
-                if (r->state == 1 && r->cancel && r->waves_queued == 0) finish_cancel(r);
+                if (pt::serve::cancel_ends_on_retire(r->state, r->cancel, r->waves_queued)) finish_cancel(r);
         } else {
             worker_error = std::string("serving wave: ") + cudaGetErrorString(e);
             for (Request* r : w.members) {
@@ -684,17 +675,24 @@ extern "C" int pt_server_cancel(pt_server* s, uint64_t ticket) {
         auto it = s->all.find(ticket);
         if (it == s->all.end()) return fail(PT_EINVAL, "unknown ticket");
         Request* r = it->second.get();
-        if (r->state == 0) {  // still queued: nothing of it is on the device
-            s->pending.erase(std::remove(s->pending.begin(), s->pending.end(), r), s->pending.end());
-            r->state = 3;
-            ++s->cancelled;
-        } else if (r->state == 1) {
-            if (r->cancel) return PT_OK;  // already being cancelled
-            r->cancel = true;
-            if (r->waves_queued == 0) s->finish_cancel(r);  // no queued wave holds its work
-            // otherwise the scheduler ends it when its last queued wave retires
-        } else {
-            return fail(PT_EINVAL, "request already finished");
+        switch (pt::serve::on_cancel(r->state, r->cancel, r->waves_queued)) {
+            case pt::serve::CancelAction::EndNow:
+                if (r->state == pt::serve::kQueued) {  // nothing of it is on the device
+                    s->pending.erase(std::remove(s->pending.begin(), s->pending.end(), r), s->pending.end());
+                    r->state = pt::serve::kCancelled;
+                    ++s->cancelled;
+                } else {  // admitted, and no queued wave holds its work
+                    r->cancel = true;
+                    s->finish_cancel(r);
+                }
+                break;
+            case pt::serve::CancelAction::EndAfterWaves:  // the scheduler ends it when its last queued wave retires
+                r->cancel = true;
+                break;
+            case pt::serve::CancelAction::AlreadyCancelling:
+                return PT_OK;
+            case pt::serve::CancelAction::Refuse:
+                return fail(PT_EINVAL, "request already finished");
         }
     }
     s->done_cv.notify_all();

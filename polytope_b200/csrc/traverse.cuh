@@ -110,8 +110,9 @@ PT_HD bool box_hits_fast(const RayState& r, float b0, float b1, float b2, float 
     const float y0 = fmul(fsub(b1, r.oy), r.iy), y1 = fmul(fsub(b4, r.oy), r.iy);
     const float z0 = fmul(fsub(b2, r.oz), r.iz), z1 = fmul(fsub(b5, r.oz), r.iz);
     const float near_t = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), 0.f));
-    const float far_t = fminf(fminf(fmul(fmaxf(x0, x1), gm), fmul(fmaxf(y0, y1), gm)),
-                              fminf(fmul(fmaxf(z0, z1), gm), min_t));
+    // the reference scales each axis's far value by 1 + 2 gamma_3 before taking the minimum;
+    // rounding is monotone and the factor positive, so scaling the minimum gives the same value
+    const float far_t = fminf(fmul(fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fmaxf(z0, z1)), gm), min_t);
     return near_t <= far_t;
 }
 
