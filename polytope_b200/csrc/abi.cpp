@@ -164,14 +164,33 @@ int scene_trace(pt_scene* s, const pt_ray* rays, uint64_t n, pt_hit* hits, uint3
     if (counted && cudaMalloc(&dcounts, 2 * sizeof(uint32_t) * n) != cudaSuccess)
         return fail(PT_ENOMEM, "cudaMalloc count buffers");
     struct Free { uint32_t* p; ~Free() { if (p) cudaFree(p); } } free_counts{dcounts};
-    const uint64_t nchunks = (n + kChunkRays - 1) / kChunkRays;
+    // Chunks: full slots in the middle, and a quarter then a half slot at both ends on long calls.
+    // The kernels wait for the first chunk's copy-in, and the last chunk's kernel and copy-out are
+    // all that runs after the final copy-in: short end chunks shorten both waits.
+    std::vector<std::pair<uint64_t, uint64_t>> chunks;  // (first ray, count)
+    if (n >= 4 * (uint64_t)kChunkRays) {
+        const uint64_t q = kChunkRays / 4, h = kChunkRays / 2;
+        chunks.push_back({0, q});
+        chunks.push_back({q, h});
+        uint64_t off = q + h;
+        while (n - off > h + q) {
+            const uint64_t cnt = std::min<uint64_t>(kChunkRays, n - off - (h + q));
+            chunks.push_back({off, cnt});
+            off += cnt;
+        }
+        chunks.push_back({off, h});
+        chunks.push_back({off + h, q});
+    } else {
+        for (uint64_t off = 0; off < n; off += kChunkRays) chunks.push_back({off, std::min<uint64_t>(kChunkRays, n - off)});
+    }
+    const uint64_t nchunks = chunks.size();
     uint64_t in_slot[kSlots];
     for (int k = 0; k < kSlots; ++k) in_slot[k] = ~0ull;  // chunk whose data occupies each slot
     auto drain = [&](int slot) -> int {  // pageable hits: move the slot's results out
         if (in_slot[slot] == ~0ull) return PT_OK;
         PT_CUDA(cudaEventSynchronize(ev_out[slot]));
         if (!pin_hits) {
-            const uint64_t off = in_slot[slot] * kChunkRays, cnt = std::min<uint64_t>(kChunkRays, n - off);
+            const uint64_t off = chunks[in_slot[slot]].first, cnt = chunks[in_slot[slot]].second;
             std::memcpy(hits + off, (pt_hit*)s->pin_out + slot * kChunkRays, cnt * sizeof(pt_hit));
         }
         in_slot[slot] = ~0ull;
@@ -184,7 +203,7 @@ int scene_trace(pt_scene* s, const pt_ray* rays, uint64_t n, pt_hit* hits, uint3
             rc = drain(slot);
             if (rc) return rc;
         }
-        const uint64_t off = c * kChunkRays, cnt = std::min<uint64_t>(kChunkRays, n - off);
+        const uint64_t off = chunks[c].first, cnt = chunks[c].second;
         pt_ray* din = (pt_ray*)s->dev_in + slot * kChunkRays;
         pt_hit* dout = (pt_hit*)s->dev_out + slot * kChunkRays;
         const void* src = rays + off;
