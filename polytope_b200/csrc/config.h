@@ -26,3 +26,13 @@
 #ifndef PT_LEAF_BATCH_WAVEFRONT
 #define PT_LEAF_BATCH_WAVEFRONT 12
 #endif
+
+// Persistent path kernel (wf_path_kernel): lanes whose ray has ended wait until this many lanes of
+// the warp can shade together (or no lane still walks), and the resident-block floor given to the
+// register allocator (blocks of 128 threads per SM).
+#ifndef PT_SHADE_BATCH_PATHS
+#define PT_SHADE_BATCH_PATHS 16
+#endif
+#ifndef PT_PATH_MIN_BLOCKS
+#define PT_PATH_MIN_BLOCKS 8
+#endif

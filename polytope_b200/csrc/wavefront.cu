@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(128) wf_shade_kernel(const WfItem* __restrict_
 // together, so the long shading code is not replayed by the warp for one or two lanes at a time.
 // Each lane's own sequence of operations is unchanged.  16 measured best on the 6.5 M-face frame
 // (with the voted walk: 1706 Msamples/s; 8: 1545, 12: 1640, 24: 1603).
-constexpr int kShadeBatch = 16;
+constexpr int kShadeBatch = PT_SHADE_BATCH_PATHS;
 
 // Per-lane path state that only the shading step reads or writes (the path's next ray, throughput,
 // radiance, bounce count, the pending shadow contribution, the slot and its pixel, sample and
@@ -265,7 +265,7 @@ struct ColdLane {
 // 1920x1080x64 frame 1840-1847 Msamples/s against 1794-1796 with that state in registers (and
 // spilled), and 1678 against 1584 Mrays/s on the 256-scene batch.
 template <int CAP, int SH>
-__global__ void __launch_bounds__(128, 8) wf_path_kernel(const WfItem* __restrict__ items, const WfSegment* __restrict__ segs,
+__global__ void __launch_bounds__(128, PT_PATH_MIN_BLOCKS) wf_path_kernel(const WfItem* __restrict__ items, const WfSegment* __restrict__ segs,
                                                       uint32_t nseg, uint32_t count, float* __restrict__ radiance,
                                                       unsigned long long* fetch, uint32_t chunk,
                                                       unsigned long long* rays_traced) {
