@@ -128,9 +128,11 @@ int pt_scene_create(const pt_scene_desc *desc, pt_scene **out);
  * and images agree in RMSE rather than bit for bit.  Shading uses the instance's world vertices
  * computed as pt_scene_create bakes them.  Primitive ids, materials, lights and the environment
  * are the flattened scene's.  The scene works with pt_trace / pt_trace_counted (node counts then
- * include top-level tests), pt_render and pt_render_rgba8 with the fused pipeline (the default
- * for such scenes; PT_RENDER_PERSISTENT and PT_RENDER_WAVEFRONT are rejected), pt_render_noalloc,
- * and batches and servers with PT_PIPELINE_FUSED.  `desc->nodes` must be NULL. */
+ * include top-level tests), pt_render and pt_render_rgba8 with the fused (default for such scenes)
+ * and persistent pipelines (PT_RENDER_WAVEFRONT is rejected), pt_render_noalloc, and batches and
+ * servers with PT_PIPELINE_PATHS or PT_PIPELINE_FUSED; every route gives the same film bit for bit.
+ * `desc->nodes` must be NULL; the top-level and bottom-level depths together must leave room in
+ * the traversal stack (PT_ESTACK otherwise). */
 int pt_scene_create_two_level(const pt_scene_desc *desc, pt_scene **out);
 
 /* What pt_scene_create_two_level would build from `desc`, computed on the host alone (no device

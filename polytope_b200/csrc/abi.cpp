@@ -456,6 +456,9 @@ int pt_scene_create_two_level(const pt_scene_desc* desc, pt_scene** out) {
     rc = prepare_two_level_host(desc, h);
     if (rc) return rc;
     if (h.tlas_depth + 2 > (uint32_t)PT_TOP_STACK) return fail(PT_ESTACK, "top-level tree too deep");
+    // the persistent path kernel keeps both levels and the instance-exit marker on one stack
+    if (h.tlas_depth + h.max_depth + 4 > (uint32_t)PT_TRAVERSAL_STACK)
+        return fail(PT_ESTACK, "top-level plus bottom-level tree depth exceeds the traversal stack");
     return create_from_host(desc, h, out);
 }
 

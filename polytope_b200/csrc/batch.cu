@@ -168,7 +168,7 @@ struct pt_batch {
     pt_batch_tuning tuning{};
     int cap = 64;
     int device = 0;
-    bool two_level = false;   // some item is a two-level scene (fused pipeline only)
+    bool two_level = false;   // some item is a two-level scene (fused or path pipeline)
     void* params = nullptr;   // RenderParams[n]
     void* items = nullptr;    // BatchItem[n]
     void* films = nullptr;    // all rgb outputs
@@ -248,6 +248,7 @@ int wf_build(pt_batch* b, const pt_batch_item* items, const pt_batch_tuning& t) 
     b->wt.queue_chunk = t.queue_chunk;
     b->wt.stack_cap = b->cap;
     b->wt.paths = t.pipeline == PT_PIPELINE_PATHS;
+    b->wt.two_level = b->two_level;
     return PT_OK;
 }
 
@@ -289,8 +290,9 @@ extern "C" int pt_batch_create(const pt_batch_item* items, uint32_t n, const pt_
             return fail(PT_EINVAL, "batch items take the batch's pipeline (no PT_RENDER_WAVEFRONT / PERSISTENT / FUSED)");
         if (i && items[i].scene->device != items[0].scene->device) return fail(PT_EINVAL, "batch items on different devices");
         if (items[i].scene->two_level) {
-            if (t.pipeline != PT_PIPELINE_FUSED)
-                return fail(PT_EINVAL, "batch item " + std::to_string(i) + ": a two-level scene needs PT_PIPELINE_FUSED");
+            if (t.pipeline == PT_PIPELINE_WAVEFRONT)
+                return fail(PT_EINVAL, "batch item " + std::to_string(i) +
+                                           ": a two-level scene needs PT_PIPELINE_PATHS or PT_PIPELINE_FUSED");
             b->two_level = true;
         }
         max_depth = std::max(max_depth, items[i].scene->max_depth);

@@ -315,6 +315,7 @@ cudaError_t pt_server::enqueue(WaveInFlight& w, const std::vector<uint32_t>& tak
         wt.queue_chunk = cfg.tuning.queue_chunk;
         wt.stack_cap = cap;
         wt.paths = cfg.tuning.pipeline == PT_PIPELINE_PATHS;
+        for (Request* r : w.members) wt.two_level = wt.two_level || r->scene->two_level;
         char* dt = (char*)d_tables;
         if (e == cudaSuccess)
             e = pt::wf_launch_wave((const pt::WfItem*)dt, (const pt::WfSegment*)(dt + ib), (const pt::WfPixels*)(dt + ib + sb),
@@ -565,8 +566,8 @@ extern "C" int pt_server_submit(pt_server* s, pt_scene* scene, const pt_render_d
     if (desc->flags & (PT_RENDER_WAVEFRONT | PT_RENDER_PERSISTENT | PT_RENDER_FUSED))
         return fail(PT_EINVAL, "served requests take the server's pipeline (no PT_RENDER_WAVEFRONT / PERSISTENT / FUSED)");
     if (scene->device != s->device) return fail(PT_EINVAL, "scene lives on another device");
-    if (scene->two_level && s->wave_engine)
-        return fail(PT_EINVAL, "a two-level scene is served by the fused pipeline only (PT_PIPELINE_FUSED)");
+    if (scene->two_level && s->cfg.tuning.pipeline == PT_PIPELINE_WAVEFRONT)
+        return fail(PT_EINVAL, "a two-level scene is served by PT_PIPELINE_PATHS or PT_PIPELINE_FUSED");
     if (!stack_cap_for(scene->max_depth, s->cfg.tuning.stack_depth)) return fail(PT_ESTACK, "tree too deep");
     std::unique_ptr<Request> r(new Request());
     r->scene = scene;

@@ -170,7 +170,8 @@ int prepare_two_level_host(const pt_scene_desc* desc, HostScene& h) {
         rc = validate_tree(t.nodes.data(), (uint32_t)t.nodes.size(), wo.num_prims, &depth);
         if (rc) return rc;
         h.max_depth = std::max(h.max_depth, depth);
-        if ((uint64_t)h.nodes.size() + t.nodes.size() > 0xFFFFFFF0ull || (uint64_t)h.tris.size() / 12 + wo.num_prims > 0xFFFFFFF0ull)
+        // bottom-level node indices share the walk stack with tagged entries (bits 30 and 31)
+        if ((uint64_t)h.nodes.size() + t.nodes.size() >= (1ull << 30) || (uint64_t)h.tris.size() / 12 + wo.num_prims > 0xFFFFFFF0ull)
             return fail(PT_EINVAL, "two-level scene too large");
         node_base.push_back((uint32_t)h.nodes.size());
         face_base.push_back((uint32_t)(h.tris.size() / 12));
@@ -189,6 +190,7 @@ int prepare_two_level_host(const pt_scene_desc* desc, HostScene& h) {
 
     // instances and their world boxes (the baked world vertices, widened by 2^-16 of their
     // magnitude: object-space hits may land a rounding step outside the baked triangles)
+    if (desc->num_meshes >= (1u << 30)) return fail(PT_EINVAL, "too many instances");
     std::vector<DeviceInstance> inst(desc->num_meshes);
     std::vector<Box> boxes(desc->num_meshes);
     for (uint32_t m = 0; m < desc->num_meshes; ++m) {

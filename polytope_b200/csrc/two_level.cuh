@@ -10,6 +10,7 @@
 #pragma once
 
 #include "instance.h"
+#include "render.h"
 #include "traverse.cuh"
 
 namespace pt {
@@ -145,6 +146,142 @@ PT_HD TwoLevelHit traverse_two_level(const TwoLevelView& v, float ox, float oy, 
         }
     }
     return out;
+}
+
+}  // namespace pt
+
+namespace pt {
+
+// ---- resumable two-level walk (the persistent path kernel) --------------------------------------
+//
+// The same walk as traverse_two_level, one node at a time, on a RayWalkT whose stack holds three
+// kinds of entries: top-level nodes (kTopTag | index), instances to enter (kInstTag | index) and
+// an exit marker (kExitTag) below each instance's bottom-level nodes (plain indices).  Entering an
+// instance carries the world ray into its object space (k.r becomes the object ray) and pushes the
+// exit marker and the instance's root; popping the marker restores the world ray.  The world ray
+// itself is kept by the caller (get_world(ox, oy, oz, dx, dy, dz)).  Visit order, box and face tests
+// and the per-ray counts are traverse_two_level's.
+constexpr uint32_t kTopTag = 0x80000000u;
+constexpr uint32_t kInstTag = 0x40000000u;
+constexpr uint32_t kExitTag = 0xFFFFFFFEu;
+
+template <int CAP, int SH>
+PT_HD void walk_begin_two_level(RayWalkT<CAP, SH>& k, float ox, float oy, float oz, float dx, float dy, float dz, float tmax,
+                                bool any, bool exact_tree) {
+    walk_begin(k, ox, oy, oz, dx, dy, dz, tmax, any, exact_tree);
+    k.stack.put(0, kTopTag);  // the top-level root
+}
+
+// A stack entry that is not a bottom-level node (bits 30 or 31 set).
+PT_HD bool two_level_tagged(uint32_t e) { return e >= kInstTag; }
+
+// Handles a tagged entry of the walk (the caller popped it): an exit marker restores the world
+// ray, an instance entry carries the ray into the instance's object space and pushes the exit
+// marker and the instance's root, a top-level node is tested like any node (its instances or its
+// children are pushed).  `lane` keeps the walk's world ray and the current instance:
+// world(ox, oy, oz, dx, dy, dz) reads the world ray, set_instance(face_base, prim_base, inst)
+// records the instance entered.  Returns 0, or -1 on a guard failure.
+template <bool COUNT, int CAP, int SH, class Lane>
+PT_HD int two_level_transition(RayWalkT<CAP, SH>& k, uint32_t e, const RenderParams* p, const Lane& lane) {
+    const bool exact = p->exact_tree != 0;
+    if (e == kExitTag) {
+        float ox, oy, oz, dx, dy, dz;
+        lane.world(ox, oy, oz, dx, dy, dz);
+        ray_setup(k.r, ox, oy, oz, dx, dy, dz);
+        k.box_mode = box_mode_for(k.r, k.min_t, exact);
+        return 0;
+    }
+    if (e & kTopTag) {
+        const uint32_t ti = e & ~kTopTag;
+        if (ti >= p->top_num_nodes) return -1;
+        uint4 a, b;
+        ldg_node((const uint4*)p->top_nodes + 2 * (size_t)ti, a, b);
+        if (COUNT) k.nodes++;
+        if (!box_test(k.r, k.box_mode, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), k.min_t))
+            return 0;
+        const uint32_t nf = b.w & 0xFFFFu;
+        if (nf > 0) {  // its instances, first one on top
+            if (k.sp + (int)nf > CAP) return -1;
+            for (uint32_t j = nf; j-- > 0;) k.stack.put(k.sp++, kInstTag | (b.z + j));
+            return 0;
+        }
+        if (k.sp + 2 > CAP) return -1;
+        const uint32_t axis = b.w >> 16;
+        const bool neg = (axis == 0 ? k.r.ix : (axis == 1 ? k.r.iy : k.r.iz)) < 0;
+        const uint32_t hi = ti + b.z, lo = ti + 1;
+        k.stack.put(k.sp++, kTopTag | (neg ? lo : hi));
+        k.stack.put(k.sp++, kTopTag | (neg ? hi : lo));
+        return 0;
+    }
+    // into an instance: the ray in its object space, then its root
+    const uint32_t ii = e & ~kInstTag;
+    const DeviceInstance* in = (const DeviceInstance*)p->instances + ii;
+    float w2o[12];
+#pragma unroll
+    for (int q = 0; q < 12; ++q) w2o[q] = ldg(in->w2o + q);
+    float ox, oy, oz, dx, dy, dz, lox, loy, loz, ldx, ldy, ldz;
+    lane.world(ox, oy, oz, dx, dy, dz);
+    to_object(w2o, ox, oy, oz, 1.0f, lox, loy, loz);
+    to_object(w2o, dx, dy, dz, 0.0f, ldx, ldy, ldz);
+    ray_setup(k.r, lox, loy, loz, ldx, ldy, ldz);
+    k.box_mode = box_mode_for(k.r, k.min_t, exact);
+    lane.set_instance(ldg(&in->face_base), ldg(&in->prim_base), ii);
+    if (k.sp + 2 > CAP) return -1;
+    k.stack.put(k.sp++, kExitTag);
+    k.stack.put(k.sp++, ldg(&in->node_base));
+    return 0;
+}
+
+// A bottom-level node step: walk_step's test on an untagged entry the caller popped; at a hit
+// leaf the faces are leaf_off .. leaf_off + leaf_n - 1 counted from the current instance's first
+// face (face_base).  Returns 1 at a hit leaf, 0 otherwise, -1 on a guard failure.
+template <bool COUNT, int CAP, int SH>
+PT_HD int two_level_node_step(RayWalkT<CAP, SH>& k, uint32_t ni, const uint4* __restrict__ nodes, uint32_t num_nodes,
+                              uint32_t& leaf_off, uint32_t& leaf_n) {
+    if (ni >= num_nodes) return -1;
+    uint4 a, b;
+    ldg_node(nodes + 2 * (size_t)ni, a, b);
+    if (COUNT) k.nodes++;
+    if (!box_test(k.r, k.box_mode, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), k.min_t))
+        return 0;
+    const uint32_t nf = b.w & 0xFFFFu;
+    if (nf > 0) {
+        leaf_off = b.z;
+        leaf_n = nf;
+        return 1;
+    }
+    if (k.sp + 2 > CAP) return -1;
+    const uint32_t axis = b.w >> 16;
+    const bool neg = (axis == 0 ? k.r.ix : (axis == 1 ? k.r.iy : k.r.iz)) < 0;
+    const uint32_t hi = ni + b.z, lo = ni + 1;
+    k.stack.put(k.sp++, neg ? lo : hi);
+    k.stack.put(k.sp++, neg ? hi : lo);
+    return 0;
+}
+
+// The faces of one bottom-level leaf (object space, records face_base + leaf_off + j); primitive
+// ids are prim_base + local face.  Returns whether a face was accepted (the caller records the
+// instance of the hit).
+template <bool COUNT, int CAP, int SH>
+PT_HD bool walk_leaf_two_level(RayWalkT<CAP, SH>& k, const float4* __restrict__ tris, uint32_t face_base, uint32_t leaf_off,
+                               uint32_t leaf_n, uint32_t prim_base) {
+    bool accepted = false;
+    for (uint32_t j = 0; j < leaf_n; ++j) {
+        const uint32_t face = face_base + leaf_off + j;
+        const size_t ti = 3 * (size_t)face;
+        const float4 q0 = ldg_face(tris + ti), q1 = ldg_face(tris + ti + 1), q2 = ldg_face(tris + ti + 2);
+        if (COUNT) k.tris++;
+        float tt, u, v, w;
+        if (wald(k.r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, k.min_t, tt, u, v, w)) {
+            k.min_t = tt;
+            k.prim = prim_base + fbits(q2.y);
+            k.leaf = face;
+            k.u = u; k.v = v; k.w = w;
+            accepted = true;
+            if (k.any) { k.done = true; return true; }
+        }
+    }
+    return accepted;
 }
 
 }  // namespace pt

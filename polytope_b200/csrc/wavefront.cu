@@ -247,7 +247,13 @@ constexpr int kShadeBatch = PT_SHADE_BATCH_PATHS;
 // banks).
 enum ColdField : uint32_t {
     kOx, kOy, kOz, kDx, kDy, kDz, kSr, kSg, kSb, kLr, kLg, kLb, kCr, kCg, kCb,
-    kBounces, kFlags, kSlot, kPixel, kSample, kItem, kColdFields
+    kBounces, kFlags, kSlot, kPixel, kSample, kItem, kColdFields,
+    // kernels that walk two-level scenes also keep the world ray of the current walk (a path ray
+    // or a shadow ray), which instance entries and exits carry in and out of object space
+    kWox = kColdFields, kWoy, kWoz, kWdx, kWdy, kWdz,
+    kFaceBase, kPrimBase, kInst,  // the instance being walked: its first face and primitive id
+    kHitInst,                     // the instance of the committed hit
+    kColdFieldsTwoLevel
 };
 constexpr uint32_t kColdShadow = 1u, kColdPending = 2u, kColdLambert = 4u, kColdExact = 8u;  // kColdExact: NaN boxes
 
@@ -261,10 +267,27 @@ struct ColdLane {
     __device__ __forceinline__ void set3(uint32_t k, const F3& v) const { set(k, v.x); set(k + 1, v.y); set(k + 2, v.z); }
 };
 
+// What two_level_transition needs of a lane: its walk's world ray and where to record the
+// instance entered, both in the lane's shared-memory fields.
+struct TwoLevelLane {
+    ColdLane cold;
+    __device__ __forceinline__ void world(float& ox, float& oy, float& oz, float& dx, float& dy, float& dz) const {
+        ox = cold.f(kWox); oy = cold.f(kWoy); oz = cold.f(kWoz);
+        dx = cold.f(kWdx); dy = cold.f(kWdy); dz = cold.f(kWdz);
+    }
+    __device__ __forceinline__ void set_instance(uint32_t face_base, uint32_t prim_base, uint32_t inst) const {
+        cold.set(kFaceBase, face_base);
+        cold.set(kPrimBase, prim_base);
+        cold.set(kInst, inst);
+    }
+};
+
 // 8 blocks of 128 per SM with the shading state in shared memory (see ColdField): on the 6.5 M-face
 // 1920x1080x64 frame 1840-1847 Msamples/s against 1794-1796 with that state in registers (and
-// spilled), and 1678 against 1584 Mrays/s on the 256-scene batch.
-template <int CAP, int SH>
+// spilled), and 1678 against 1584 Mrays/s on the 256-scene batch.  TL: the wave may hold
+// two-level scenes (a lane walks its item's layout: walk_step, or two_level_node_step and
+// two_level_transition).
+template <int CAP, int SH, bool TL>
 __global__ void __launch_bounds__(128, PT_PATH_MIN_BLOCKS) wf_path_kernel(const WfItem* __restrict__ items, const WfSegment* __restrict__ segs,
                                                       uint32_t nseg, uint32_t count, float* __restrict__ radiance,
                                                       unsigned long long* fetch, uint32_t chunk,
@@ -273,9 +296,23 @@ __global__ void __launch_bounds__(128, PT_PATH_MIN_BLOCKS) wf_path_kernel(const 
     const uint32_t lt_mask = (1u << lane) - 1u;
     const float inf = bitsf(0x7F800000u);
     __shared__ uint32_t sstack[SH > 0 ? SH * 128 : 1];
-    __shared__ uint32_t scold[kColdFields * 128];
+    __shared__ uint32_t scold[(TL ? kColdFieldsTwoLevel : kColdFields) * 128];
     const ColdLane cold{scold + threadIdx.x};
     RayWalkT<CAP, SH> k;
+    // two-level lanes: the instance bookkeeping lives in the lane's shared fields, so the
+    // bottom-level node steps carry no extra registers
+    bool two = false;
+    const TwoLevelLane tl_lane{cold};
+    // starts a walk of the lane's ray in its item's layout
+    auto begin = [&](const F3& o, const F3& d, float tmax, bool any, bool exact) {
+        if (TL && two) {
+            cold.set3(kWox, o);
+            cold.set3(kWdx, d);
+            walk_begin_two_level(k, o.x, o.y, o.z, d.x, d.y, d.z, tmax, any, exact);
+        } else {
+            walk_begin(k, o.x, o.y, o.z, d.x, d.y, d.z, tmax, any, exact);
+        }
+    };
     k.stack.base = sstack + threadIdx.x;
     k.stack.stride = 128;
     uint32_t pool_next = 0, pool_end = 0;
@@ -322,7 +359,8 @@ __global__ void __launch_bounds__(128, PT_PATH_MIN_BLOCKS) wf_path_kernel(const 
                 cold.set(kPixel, pixel);
                 cold.set(kSample, sample);
                 cold.set(kItem, item);
-                walk_begin(k, o.x, o.y, o.z, d.x, d.y, d.z, inf, false, exact);
+                if (TL) two = p->instances != nullptr;
+                begin(o, d, inf, false, exact);
                 active = true;
                 finished = false;
             }
@@ -336,7 +374,32 @@ __global__ void __launch_bounds__(128, PT_PATH_MIN_BLOCKS) wf_path_kernel(const 
         {
             uint32_t leaf_off = 0, leaf_n = 0;
             bool ok, at_leaf;
-            if constexpr (PT_LEAF_BATCH_PATHS > 0) {
+            if constexpr (TL) {
+                // walk_round with each lane stepping its own layout
+                at_leaf = false;
+                ok = true;
+                const bool walking0 = active && !finished && k.sp > 0;
+                const uint32_t cand = __ballot_sync(0xFFFFFFFFu, walking0);
+                const int want = __popc(cand) < PT_LEAF_BATCH_PATHS ? __popc(cand) : PT_LEAF_BATCH_PATHS;
+                while (true) {
+                    const bool w_now = walking0 && ok && !at_leaf && k.sp > 0;
+                    const uint32_t w = __ballot_sync(0xFFFFFFFFu, w_now);
+                    if (w == 0 || __popc(cand & ~w) >= want) break;
+                    if (w_now) {
+                        int r;
+                        if (two) {
+                            const uint32_t e = k.stack.get(--k.sp);
+                            r = two_level_tagged(e)
+                                    ? two_level_transition<false>(k, e, items[cold.u(kItem)].params, tl_lane)
+                                    : two_level_node_step<false>(k, e, nodes, num_nodes, leaf_off, leaf_n);
+                        } else {
+                            r = walk_step<false>(k, nodes, num_nodes, leaf_off, leaf_n);
+                        }
+                        at_leaf = r > 0;
+                        ok = r >= 0;
+                    }
+                }
+            } else if constexpr (PT_LEAF_BATCH_PATHS > 0) {
                 walk_round<false, 1>(k, active && !finished && k.sp > 0, PT_LEAF_BATCH_PATHS, nodes, num_nodes, at_leaf,
                                      ok, leaf_off, leaf_n);
             } else {
@@ -344,7 +407,14 @@ __global__ void __launch_bounds__(128, PT_PATH_MIN_BLOCKS) wf_path_kernel(const 
                 ok = !walking || walk_to_leaf<false>(k, nodes, num_nodes, leaf_off, leaf_n);
                 at_leaf = walking && ok && leaf_n > 0;
             }
-            if (at_leaf) walk_leaf<false>(k, tris, leaf_off, leaf_n);
+            if (at_leaf) {
+                if (TL && two) {
+                    if (walk_leaf_two_level<false>(k, tris, cold.u(kFaceBase), leaf_off, leaf_n, cold.u(kPrimBase)))
+                        cold.set(kHitInst, cold.u(kInst));
+                } else {
+                    walk_leaf<false>(k, tris, leaf_off, leaf_n);
+                }
+            }
             if (active && !finished && (!ok || k.done || k.sp == 0)) {
                 finished = true;
                 walk_ok = ok;
@@ -375,7 +445,10 @@ __global__ void __launch_bounds__(128, PT_PATH_MIN_BLOCKS) wf_path_kernel(const 
                     const uint32_t pixel = cold.u(kPixel), sample = cold.u(kSample);
                     if (s.bounces == 0 && sample == 0 && it.primary) it.primary[pixel] = k.prim;
                     ShadowReq sh;
-                    const bool more = shade_hit(*p, s, k.prim, k.leaf, k.u, k.v, k.w, pixel, sample, sh);
+                    const bool more = (TL && two)
+                                          ? shade_hit_two_level(*p, s, k.prim, k.leaf, cold.u(kHitInst), k.u, k.v, k.w, pixel,
+                                                                sample, sh)
+                                          : shade_hit(*p, s, k.prim, k.leaf, k.u, k.v, k.w, pixel, sample, sh);
                     cold.set3(kOx, s.o);
                     cold.set3(kDx, s.d);
                     cold.set3(kSr, s.src);
@@ -386,7 +459,7 @@ __global__ void __launch_bounds__(128, PT_PATH_MIN_BLOCKS) wf_path_kernel(const 
                         cold.set3(kCr, sh.contrib);
                         flags |= kColdShadow | (more ? kColdPending : 0u);
                         next_shadow = true;
-                        walk_begin(k, sh.o.x, sh.o.y, sh.o.z, sh.wi.x, sh.wi.y, sh.wi.z, sh.tmax, true, exact);
+                        begin(sh.o, sh.wi, sh.tmax, true, exact);
                     } else {
                         go = more && !throughput_is_zero(s.src);
                     }
@@ -398,8 +471,7 @@ __global__ void __launch_bounds__(128, PT_PATH_MIN_BLOCKS) wf_path_kernel(const 
                 }
                 if (!next_shadow) {
                     if (go) {
-                        const F3 o = cold.f3at(kOx), d = cold.f3at(kDx);
-                        walk_begin(k, o.x, o.y, o.z, d.x, d.y, d.z, inf, false, exact);
+                        begin(cold.f3at(kOx), cold.f3at(kDx), inf, false, exact);
                     } else {
                         clamp_store(radiance + 3 * (size_t)cold.u(kSlot), cold.f3at(kLr));
                         active = false;
@@ -594,14 +666,14 @@ cudaError_t launch_trace_stage(const WfItem* items, const WfState& ws, const uin
     return cudaGetLastError();
 }
 
-template <int CAP>
+template <int CAP, bool TL>
 cudaError_t launch_path_stage(const WfItem* items, const WfSegment* segs, uint32_t nseg, uint32_t count, float* radiance,
                               unsigned long long* fetch, uint32_t chunk, unsigned long long* rays, cudaStream_t s) {
     constexpr int SH = 16;
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wf_path_kernel<CAP, SH>, 128, 0);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, wf_path_kernel<CAP, SH, TL>, 128, 0);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) per_sm = 1;
     uint64_t grid = (uint64_t)sms * per_sm;
@@ -609,17 +681,20 @@ cudaError_t launch_path_stage(const WfItem* items, const WfSegment* segs, uint32
     if (grid > grid_needed) grid = grid_needed ? grid_needed : 1;
     e = cudaMemsetAsync(fetch, 0, sizeof(unsigned long long), s);
     if (e != cudaSuccess) return e;
-    wf_path_kernel<CAP, SH><<<(unsigned)grid, 128, 0, s>>>(items, segs, nseg, count, radiance, fetch, chunk, rays);
+    wf_path_kernel<CAP, SH, TL><<<(unsigned)grid, 128, 0, s>>>(items, segs, nseg, count, radiance, fetch, chunk, rays);
     return cudaGetLastError();
 }
 
-cudaError_t path_stage(int cap, const WfItem* items, const WfSegment* segs, uint32_t nseg, uint32_t count, float* radiance,
-                       unsigned long long* fetch, uint32_t chunk, unsigned long long* rays, cudaStream_t s) {
+cudaError_t path_stage(int cap, bool two_level, const WfItem* items, const WfSegment* segs, uint32_t nseg, uint32_t count,
+                       float* radiance, unsigned long long* fetch, uint32_t chunk, unsigned long long* rays, cudaStream_t s) {
+    if (two_level) {  // the top level, the exit marker and the bottom level share the stack: the largest capacity
+        return launch_path_stage<64, true>(items, segs, nseg, count, radiance, fetch, chunk, rays, s);
+    }
     switch (cap) {
-        case 24: return launch_path_stage<24>(items, segs, nseg, count, radiance, fetch, chunk, rays, s);
-        case 32: return launch_path_stage<32>(items, segs, nseg, count, radiance, fetch, chunk, rays, s);
-        case 48: return launch_path_stage<48>(items, segs, nseg, count, radiance, fetch, chunk, rays, s);
-        default: return launch_path_stage<64>(items, segs, nseg, count, radiance, fetch, chunk, rays, s);
+        case 24: return launch_path_stage<24, false>(items, segs, nseg, count, radiance, fetch, chunk, rays, s);
+        case 32: return launch_path_stage<32, false>(items, segs, nseg, count, radiance, fetch, chunk, rays, s);
+        case 48: return launch_path_stage<48, false>(items, segs, nseg, count, radiance, fetch, chunk, rays, s);
+        default: return launch_path_stage<64, false>(items, segs, nseg, count, radiance, fetch, chunk, rays, s);
     }
 }
 
@@ -668,8 +743,8 @@ cudaError_t wf_launch_wave(const WfItem* d_items, const WfSegment* d_segments, c
     if (w.count == 0) return cudaSuccess;
     if (w.count > ws.capacity) return cudaErrorInvalidValue;
     if (!t.paths && !ws.ray_o) return cudaErrorInvalidValue;  // state carved for the path kernel only
-    cudaError_t e = t.paths ? path_stage(t.stack_cap, d_items, d_segments + w.seg_begin, w.seg_count, w.count, ws.radiance,
-                                         (unsigned long long*)(ws.counters + 4), t.queue_chunk, rays_traced, s)
+    cudaError_t e = t.paths ? path_stage(t.stack_cap, t.two_level, d_items, d_segments + w.seg_begin, w.seg_count, w.count,
+                                         ws.radiance, (unsigned long long*)(ws.counters + 4), t.queue_chunk, rays_traced, s)
                             : bounce_stages(d_items, d_segments, w, ws, t, rays_traced, s);
     if (e != cudaSuccess) return e;
     if (w.res_pixels)

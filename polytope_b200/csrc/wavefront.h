@@ -75,6 +75,7 @@ struct WfTuning {
     uint32_t queue_chunk = 64;         // rays a warp takes per fetch in the persistent kernels
     int stack_cap = 64;                // traversal stack entries
     bool paths = false;                // one thread per whole path instead of per-bounce kernels
+    bool two_level = false;            // (paths only) some item is a two-level scene
 };
 
 // One wave: `count` slots, `bounces` extend/shade/shadow iterations, and its ranges in the plan's

@@ -9,8 +9,9 @@ which is itself bit-exact with the reference:
   * t of equal ids agrees to T_REL (1e-5) relative; any-hit outcomes agree on >= 99.9 % of rays;
   * films at equal spp agree within REL_RMSE_TOL relative RMSE and MEAN_TOL relative mean absolute
     error, primary ids on >= 99.9 % of pixels;
-  * the same two-level frame is bit-identical through pt_render, a batch and the serving loop
-    (they run the same fused path code).
+  * the same two-level frame is bit-identical through pt_render's fused (default) and persistent
+    pipelines, batches and the serving loop on the fused and path pipelines, pt_render_noalloc and
+    pt_render_rgba8 (the persistent kernel's resumable walk makes the fused kernel's hits).
 Scene: the instanced workload (the displaced sphere instanced five times with seeded rigid
 transforms, Lambert or mirror, over a ground quad, a 3x3 light, environment 0.2)."""
 import numpy as np
@@ -105,27 +106,37 @@ def test_two_level_render_matches_the_flattened_film(scenes):
     assert b.mean() > 1.0
 
 
-def test_two_level_frame_is_the_same_through_every_fused_route(scenes):
+def test_two_level_frame_is_the_same_through_every_route(scenes):
+    """The persistent path kernel's resumable two-level walk (walk_step_two_level) and the fused
+    kernel's traverse_two_level make the same hits, so a two-level frame is bit-identical through
+    pt_render's default and fused pipelines, batches and the serving loop on both their pipelines
+    (mixed with a flattened item), pt_render_noalloc and pt_render_rgba8."""
     import ctypes as C
     import torch
     meshes, env, flat, two = scenes
-    rd = pb.render_desc(64, 48, 4, 6, W.INSTANCED_CAMERA, 5, pb.RENDER_NEE | pb.RENDER_JITTER)
-    rgb, prim = pb.render(two, 64, 48, 4, 6, W.INSTANCED_CAMERA, 5, pb.RENDER_NEE | pb.RENDER_JITTER)
-    f_rgb, _ = pb.render(flat, 64, 48, 4, 6, W.INSTANCED_CAMERA, 5, pb.RENDER_NEE | pb.RENDER_JITTER)
-    t = pb.default_tuning()
-    t.pipeline = pb.PIPELINE_FUSED
-    b = pb.Batch([(two, rd), (flat, rd)], t)  # a two-level and a flattened item in one launch
-    b.run()
-    assert_bit_equal(b.output(0)[0], rgb, "batch, two-level item")
-    assert_bit_equal(b.output(0)[1], prim, "batch, two-level primary ids")
-    assert_bit_equal(b.output(1)[0], f_rgb, "batch, flattened item")
-    b.close()
-    srv = pb.Server(max_inflight=4, wave_pixels=1 << 12, tuning=t)
-    tk = [srv.submit(two, rd), srv.submit(flat, rd)]
-    assert srv.wait(tk[0], 60000) == pb.REQ_DONE and srv.wait(tk[1], 60000) == pb.REQ_DONE
-    assert_bit_equal(srv.fetch(tk[0])[0], rgb, "served, two-level")
-    assert_bit_equal(srv.fetch(tk[1])[0], f_rgb, "served, flattened")
-    srv.close()
+    fl = pb.RENDER_NEE | pb.RENDER_JITTER
+    rd = pb.render_desc(64, 48, 4, 6, W.INSTANCED_CAMERA, 5, fl)
+    rgb, prim = pb.render(two, 64, 48, 4, 6, W.INSTANCED_CAMERA, 5, fl | pb.RENDER_FUSED)
+    for name, extra, wave in (("default", 0, 0), ("persistent", pb.RENDER_PERSISTENT, 0), ("persistent, small waves", 0, 1000)):
+        r2, p2 = pb.render(two, 64, 48, 4, 6, W.INSTANCED_CAMERA, 5, fl | extra, wave)
+        assert_bit_equal(r2, rgb, f"pt_render {name}")
+        assert_bit_equal(p2, prim, f"pt_render {name} primary ids")
+    f_rgb, _ = pb.render(flat, 64, 48, 4, 6, W.INSTANCED_CAMERA, 5, fl)
+    for pipe in (pb.PIPELINE_FUSED, pb.PIPELINE_PATHS):
+        t = pb.default_tuning()
+        t.pipeline = pipe
+        b = pb.Batch([(two, rd), (flat, rd)], t)  # a two-level and a flattened item in one launch
+        b.run()
+        assert_bit_equal(b.output(0)[0], rgb, f"batch {pipe}, two-level item")
+        assert_bit_equal(b.output(0)[1], prim, f"batch {pipe}, two-level primary ids")
+        assert_bit_equal(b.output(1)[0], f_rgb, f"batch {pipe}, flattened item")
+        b.close()
+        srv = pb.Server(max_inflight=4, wave_pixels=1 << 12, tuning=t)
+        tk = [srv.submit(two, rd), srv.submit(flat, rd)]
+        assert srv.wait(tk[0], 60000) == pb.REQ_DONE and srv.wait(tk[1], 60000) == pb.REQ_DONE
+        assert_bit_equal(srv.fetch(tk[0])[0], rgb, f"served {pipe}, two-level")
+        assert_bit_equal(srv.fetch(tk[1])[0], f_rgb, f"served {pipe}, flattened")
+        srv.close()
     out = torch.full((64 * 48 * 3,), float("nan"), dtype=torch.float32, device="cuda")
     pb.check(pb.lib.pt_render_noalloc(two.handle, C.byref(rd), out.data_ptr(), None, None))
     torch.cuda.synchronize()
@@ -135,14 +146,13 @@ def test_two_level_frame_is_the_same_through_every_fused_route(scenes):
     assert_bit_equal(rgba, po.film_to_rgba8(rgb), "pt_render_rgba8")
 
 
-def test_two_level_scene_refuses_the_other_pipelines(scenes):
+def test_two_level_scene_refuses_the_wavefront_pipeline(scenes):
     meshes, env, flat, two = scenes
-    for fl in (pb.RENDER_PERSISTENT, pb.RENDER_WAVEFRONT):
-        with pytest.raises(pb.PolytopeError) as e:
-            pb.render(two, 8, 8, 1, 2, W.INSTANCED_CAMERA, 1, fl)
-        assert e.value.code == pb.PT_EINVAL
+    with pytest.raises(pb.PolytopeError) as e:
+        pb.render(two, 8, 8, 1, 2, W.INSTANCED_CAMERA, 1, pb.RENDER_WAVEFRONT)
+    assert e.value.code == pb.PT_EINVAL
     rd = pb.render_desc(8, 8, 1, 2, W.INSTANCED_CAMERA)
-    for pipe in (pb.PIPELINE_WAVEFRONT, pb.PIPELINE_PATHS):
+    for pipe in (pb.PIPELINE_WAVEFRONT,):
         t = pb.default_tuning()
         t.pipeline = pipe
         with pytest.raises(pb.PolytopeError) as e:
