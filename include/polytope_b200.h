@@ -18,6 +18,13 @@
  *                                                                   src/cpu/runners/TileRunner.cpp:77-117,
  *                                                                   src/cpu/runners/AbstractRunner.cpp:11-31,
  *                                                                   src/cpu/integrators/PathTraceIntegrator.cpp:10-135
+ *   pt_render_rgba8   <- the same, then Output()'s PNGFilm quantisation src/cpu/films/PNGFilm.cpp:20-45
+ *   pt_load_ply / pt_load_obj / pt_load_pbrt, pt_film_to_rgba8 / pt_write_png
+ *                     <- the scene readers and the PNG output step (declared below with their citations)
+ *
+ * Entry points with no counterpart in the reference (one frame per process, no instancing layout,
+ * errors end the process): pt_scene_status, pt_render_noalloc, pt_scene_create_two_level,
+ * pt_two_level_plan, pt_batch_*, pt_tuning_*, pt_server_* (pt_server_cancel among them).
  *
  * Conventions
  *   - Every function returns PT_OK (0) or a negative PT_E* status and never exits the process

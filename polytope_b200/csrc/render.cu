@@ -1,11 +1,14 @@
 // render.cu -- the render call (TileRunner::Run + AbstractRunner::Trace + PathTraceIntegrator)
 // as sm_100a kernels.  Paths are numbered sample-major (path = sample * W*H + pixel) and rendered
-// in waves.  Two pipelines compute identical results:
-//   * fused:     one thread runs a whole path (camera ray, bounces, shadow rays);
+// in waves.  Three pipelines compute identical results:
+//   * persistent (the default): one persistent path kernel per wave (wavefront.cu wf_path_kernel)
+//                whose lanes take the next path as soon as theirs ends;
+//   * fused:     one thread runs a whole path (camera ray, bounces, shadow rays), one launch per
+//                wave (path_kernel below; the default for two-level scenes);
 //   * wavefront: per bounce an extend kernel (closest hit) over a compacted queue, a shade kernel
 //                that appends the next rays and the shadow rays to queues with warp-vote
 //                compaction and one atomic per warp, and a shadow kernel (any hit).
-// Either way a resolve kernel then adds each pixel's samples to the film in sample order (the
+// Each way a resolve kernel then adds each pixel's samples to the film in sample order (the
 // order of BoxFilter::Output's sum, BoxFilter.cpp:54-71), so the film is deterministic and equal
 // to the CPU oracle's bit for bit.
 
