@@ -72,8 +72,16 @@ __global__ void __launch_bounds__(128) wf_init_kernel(const WfItem* __restrict__
 // registers by 9 %, and 3 blocks or 5-6 blocks are slower; 16 shared entries together with the
 // warp-voted walk (PT_LEAF_BATCH_WAVEFRONT) gave 2024 Mrays/s against 1806 for neither (8 or 24
 // entries: 1918 / 1954 at batch 16; shared entries without the vote: no gain).
-constexpr int kWfTraceShared = 16;
-constexpr int kWfTraceMinBlocks = 4;
+// Re-swept with the min/max box test (256-scene batch, Mrays/s): leaf batch 12 / 16 / 8: 2199 /
+// 2150 / 2121; 24 shared entries: 2198; 3 / 5 blocks per SM: 1967 / 1842.
+#ifndef PT_WF_TRACE_SHARED
+#define PT_WF_TRACE_SHARED 16
+#endif
+#ifndef PT_WF_TRACE_MIN_BLOCKS
+#define PT_WF_TRACE_MIN_BLOCKS 4
+#endif
+constexpr int kWfTraceShared = PT_WF_TRACE_SHARED;
+constexpr int kWfTraceMinBlocks = PT_WF_TRACE_MIN_BLOCKS;
 
 template <int CAP, bool SHADOW>
 __global__ void __launch_bounds__(256, kWfTraceMinBlocks) wf_trace_kernel(const WfItem* __restrict__ items, WfState ws,
