@@ -268,6 +268,7 @@ def serve_requests(pb, n_scenes, n_requests, seed):
 def serve_tuning(pb):
     t = pb.default_tuning()
     t.pipeline = pb.PIPELINE_PATHS
+    t.queue_chunk = 128  # the persistent path kernel's best chunk with 32 M-path waves (as pt_render's default)
     return t
 
 
