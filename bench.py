@@ -369,7 +369,7 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
                      "films by DMA into a 2 GiB pinned arena; a client thread copies results out in submission order "
                      "into reused buffers (the plain arm renders into the same reused buffers)",
            "timing": "host steady clock from the first arrival to the last completion (film in host memory); latency = completion - arrival; "
-                     "each arm's run with the median makespan of 3 (runs: [Mrays/s, p99 ms(, GPU busy ms of the waves)] of each)",
+                     "each arm's run with the median makespan of 3 (runs: [Mrays/s, p99 ms(, GPU busy ms of the waves, scheduler planning ms)] of each)",
            "rates": [],
            "pool": {"faces": int(sum(sum(len(m.faces) for m in sp[0]) for sp in pool)),
                     "device_bytes": int(sum(sc.info().device_bytes for sc in scenes)),
@@ -395,6 +395,8 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
             served[-1]["gpu_busy_ms"] = round(s1["busy_ms"] - s0["busy_ms"], 1)
             served[-1]["waves"] = int(s1["waves"] - s0["waves"])
             served[-1]["blocked_admission_ms"] = round(s1["blocked_ms"] - s0["blocked_ms"], 1)
+            served[-1]["scheduler_plan_ms"] = round(s1["plan_ms"] - s0["plan_ms"], 1)
+            served[-1]["scheduler_retire_wait_ms"] = round(s1["retire_wait_ms"] - s0["retire_wait_ms"], 1)
             served[-1]["admission_wait_ms"] = {"p50": pct(run_served.admission_ms, 50), "p99": pct(run_served.admission_ms, 99)}
             lat_p, span_p = run_plain(pb, scenes, reqs, arrivals, films)
             plain.append(summary(lat_p, span_p, rays))
@@ -404,7 +406,7 @@ def bench_served(pb, torch, n_scenes=32, n_requests=300, rates=(50.0, 200.0, 200
         med = lambda runs: sorted(runs, key=lambda r: r["makespan_s"])[len(runs) // 2]
         out["rays"] = int(rays)
         entry = {"rate_per_s": rate, "served": med(served), "plain_per_request": med(plain),
-                 "runs": {"served": [(r["mrays_s"], r["p99_ms"], r["gpu_busy_ms"]) for r in served],
+                 "runs": {"served": [(r["mrays_s"], r["p99_ms"], r["gpu_busy_ms"], r["scheduler_plan_ms"]) for r in served],
                           "plain_per_request": [(r["mrays_s"], r["p99_ms"]) for r in plain]}}
         entry["served_over_plain"] = round(entry["served"]["mrays_s"] / entry["plain_per_request"]["mrays_s"], 3)
         if top:

@@ -42,7 +42,10 @@ using Clock = std::chrono::steady_clock;
 
 namespace {
 
-constexpr int kWavesQueued = 2;  // waves enqueued on the stream at once (host planning overlaps the GPU)
+#ifndef PT_SERVE_WAVES_QUEUED
+#define PT_SERVE_WAVES_QUEUED 2
+#endif
+constexpr int kWavesQueued = PT_SERVE_WAVES_QUEUED;  // waves enqueued on the stream at once (host planning overlaps the GPU)
 
 // A request; its scheduling state (state, cancel, total and planned work units -- pixels for the
 // fused pipeline, sample-major paths for the wave pipelines) is the serve::Work base.
@@ -536,6 +539,17 @@ extern "C" int pt_server_create(const pt_server_config* cfg, pt_server** out) {
         // to the driver at every synchronisation
         uint64_t keep = ~0ull;
         cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        // and map the first min(budget, 4 GiB) now (64 in-flight 1024^2 requests hold about
+        // 1.8 GiB), so that admissions take memory the pool already has instead of growing it on
+        // the scheduler thread while the queued waves run dry
+        const size_t prime = (size_t)std::min<uint64_t>(s->cfg.memory_budget, 4ull << 30);
+        void* block = nullptr;
+        if (prime && cudaMallocFromPoolAsync(&block, prime, s->pool, s->stream) == cudaSuccess) {
+            cudaFreeAsync(block, s->stream);
+            cudaStreamSynchronize(s->stream);
+        } else {
+            cudaGetLastError();  // the pool then grows on demand, as before
+        }
     }
     if (ok && s->wave_engine) {
         const uint64_t cap_paths = std::min<uint64_t>(s->cfg.wave_pixels, 1ull << 26);
