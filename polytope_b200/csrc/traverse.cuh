@@ -104,8 +104,58 @@ PT_HD bool box_hits(const RayState& r, float b0, float b1, float b2, float b3, f
 // : b` are min / max up to the sign of a zero, which the final `near <= far` comparison does not
 // see.  So one min / max instruction replaces each compare-and-select, and the inside early-out is
 // skipped as in box_hits (needs_inside_test is false for such rays when tmax >= 0).
+#ifndef PT_PACKED_BOX
+#define PT_PACKED_BOX 1
+#endif
+#if defined(__CUDA_ARCH__) && PT_PACKED_BOX
+// sm_100 packed single-precision arithmetic: sub / mul .rn.f32x2 round each half exactly as the
+// scalar __fsub_rn / __fmul_rn (no flush of subnormals), and three-input min / max.  The fast box
+// test drops from 26 to 18 instructions; measured on a B200 (two runs each, same box): 1.3 M-face
+// ray queries 2176 vs 2142 Mrays/s, the 6.5 M-face frame 1782 vs 1763 Msamples/s, the 256-scene
+// batch 2248-2262 vs 2210-2226 Mrays/s, with the same hits and films.
+__device__ __forceinline__ uint64_t pack2(float lo, float hi) {
+    uint64_t v;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(v) : "f"(lo), "f"(hi));
+    return v;
+}
+__device__ __forceinline__ void unpack2(uint64_t v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ uint64_t sub2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ uint64_t mul2(uint64_t a, uint64_t b) {
+    uint64_t d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float d;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+#endif
+
 PT_HD bool box_hits_fast(const RayState& r, float b0, float b1, float b2, float b3, float b4, float b5, float min_t) {
     const float gm = bitsf(PT_GAMMA_MUL_BITS);
+#if defined(__CUDA_ARCH__) && PT_PACKED_BOX
+    // the six slab products as three packed pairs: (x0, y0), (z0, x1), (y1, z1), the box words
+    // taken in record order (b0 b1 | b2 b3 | b4 b5)
+    float x0, y0, z0, x1, y1, z1;
+    unpack2(mul2(sub2(pack2(b0, b1), pack2(r.ox, r.oy)), pack2(r.ix, r.iy)), x0, y0);
+    unpack2(mul2(sub2(pack2(b2, b3), pack2(r.oz, r.ox)), pack2(r.iz, r.ix)), z0, x1);
+    unpack2(mul2(sub2(pack2(b4, b5), pack2(r.oy, r.oz)), pack2(r.iy, r.iz)), y1, z1);
+    const float near_t = fmaxf(max3f(fminf(x0, x1), fminf(y0, y1), fminf(z0, z1)), 0.f);
+    const float far_t = fminf(fmul(min3f(fmaxf(x0, x1), fmaxf(y0, y1), fmaxf(z0, z1)), gm), min_t);
+    return near_t <= far_t;
+#else
     const float x0 = fmul(fsub(b0, r.ox), r.ix), x1 = fmul(fsub(b3, r.ox), r.ix);
     const float y0 = fmul(fsub(b1, r.oy), r.iy), y1 = fmul(fsub(b4, r.oy), r.iy);
     const float z0 = fmul(fsub(b2, r.oz), r.iz), z1 = fmul(fsub(b5, r.oz), r.iz);
@@ -114,6 +164,7 @@ PT_HD bool box_hits_fast(const RayState& r, float b0, float b1, float b2, float 
     // rounding is monotone and the factor positive, so scaling the minimum gives the same value
     const float far_t = fminf(fmul(fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fmaxf(z0, z1)), gm), min_t);
     return near_t <= far_t;
+#endif
 }
 
 // Which box test a ray takes (walk state box_mode): 0 box_hits_fast, 1 box_hits without the inside
