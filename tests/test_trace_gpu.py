@@ -63,6 +63,30 @@ def test_box_test_on_device_matches_reference_semantics(cuda_device):
     assert (got.astype(bool) == exp).all(), np.nonzero(got.astype(bool) != exp)[0][:10]
 
 
+def test_box_test_on_device_keeps_subnormals(cuda_device):
+    """The min/max box test of finite rays (packed f32x2 slab products on the device) on boxes,
+    origins and far bounds of subnormal size, where flushing a difference or a product to zero
+    would change the answer (it would on 86 % of these cases); unit directions aimed near each
+    box, so about one case in seven hits."""
+    rng = np.random.default_rng(23)
+    n = 20000
+    tiny = np.float32(1e-39)  # below FLT_MIN (1.18e-38)
+    lo = (rng.uniform(-2, 1, (n, 3)) * tiny).astype(np.float32)
+    hi = (lo + rng.uniform(0, 2, (n, 3)).astype(np.float32) * tiny).astype(np.float32)
+    o = (rng.uniform(-3, 3, (n, 3)) * tiny).astype(np.float32)
+    aim = ((lo + hi) / 2 - o).astype(np.float64) + rng.normal(size=(n, 3)) * 1e-39
+    d = (aim / np.linalg.norm(aim, axis=1)[:, None]).astype(np.float32)
+    d[d == 0] = np.float32(1e-20)
+    tmax = rng.choice(np.array([np.inf, 1e-39, 5e-40, 1e-30, 1.0], np.float32), n).astype(np.float32)
+    case = np.zeros((n, 16), np.float32)
+    case[:, 0:3], case[:, 3:6], case[:, 6:9], case[:, 9:12], case[:, 12] = lo, hi, o, d, tmax
+    assert (np.abs(case[:, 0:9]) < 1.18e-38).mean() > 0.9
+    got = pb.selftest_device(3, case, n)
+    exp = np.array([po.bbox_hits("orc", np.concatenate([lo[i], hi[i]]), o[i], d[i], float(tmax[i])) for i in range(n)])
+    assert 0.05 < exp.mean() < 0.95, exp.mean()
+    assert (got.astype(bool) == exp).all(), np.nonzero(got.astype(bool) != exp)[0][:10]
+
+
 def test_small_scene_random_rays_match_fixture_and_oracle(cuda_device):
     g = load_golden("small_scene.npz")
     meshes, env = W.small_scene()
