@@ -116,26 +116,36 @@ def bench_batched(pb, torch, n_scenes=256):
             for sc, (_, _, d) in zip(scenes, work)]
     fused = [(sc, pb.render_desc(d["width"], d["height"], d["spp"], d["max_depth"], d["camera"], d["seed"],
                                  pb.RENDER_NEE | pb.RENDER_FUSED)) for sc, (_, _, d) in zip(scenes, work)]
+    wavefront = [(sc, pb.render_desc(d["width"], d["height"], d["spp"], d["max_depth"], d["camera"], d["seed"],
+                                     pb.RENDER_NEE | pb.RENDER_WAVEFRONT)) for sc, (_, _, d) in zip(scenes, work)]
     outs = [torch.empty(rd.width * rd.height * 3, dtype=torch.float32, device="cuda") for _, rd in jobs]
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
-    def plain(js):
+    def plain(js, per_frame=None):
         # pt_render with device films only queues its work, so the events bracket the GPU time of
         # 256 back-to-back frames on the stream
         for (sc, rd), o in zip(js[:8], outs):
             pb.check(pb.lib.pt_render(sc.handle, C.byref(rd), o.data_ptr(), None, pb.MEM_DEVICE, None))
         torch.cuda.synchronize()
+        marks = [torch.cuda.Event(enable_timing=True) for _ in js] if per_frame is not None else []
         e0.record()
-        for (sc, rd), o in zip(js, outs):
+        for k, ((sc, rd), o) in enumerate(zip(js, outs)):
             pb.check(pb.lib.pt_render(sc.handle, C.byref(rd), o.data_ptr(), None, pb.MEM_DEVICE, None))
+            if marks:
+                marks[k].record()
         e1.record()
         e1.synchronize()
         for sc, _ in js[:1]:
             assert sc.status() == pb.PT_OK
+        if marks:
+            per_frame[:] = [e0.elapsed_time(marks[0])] + [a.elapsed_time(b) for a, b in zip(marks, marks[1:])]
         return e0.elapsed_time(e1)
 
-    plain_ms = plain(jobs)
+    frame_ms, frame_wf_ms = [], []
+    plain_ms = plain(jobs, frame_ms)
     fused_ms = plain(fused)
+    wavefront_ms = plain(wavefront, frame_wf_ms)
+    best_pick_ms = sum(min(a, b) for a, b in zip(frame_ms, frame_wf_ms))
     best, _, trials = pb.autotune(jobs[::8])
     b = pb.Batch(jobs, best)
     b.run()
@@ -146,16 +156,44 @@ def bench_batched(pb, torch, n_scenes=256):
     batch_ms = e0.elapsed_time(e1)
     rays = b.rays_traced()
     b.close()
+    # How much of the plain arm's time is the GPU left underfilled by small frames?  Each frame's
+    # rays (one-item batches, untimed: the same rays as pt_render's) against its own plain time;
+    # frames of at least 4,194,304 paths fill the GPU many times over and set the plain kernel's
+    # full rate on these scenes.  At that rate for every frame the plain arm would take ideal_ms,
+    # the most that batching alone (filling the GPU) can recover.
+    frame_rays = []
+    for job in jobs:
+        one = pb.Batch([job])
+        one.run()
+        frame_rays.append(one.rays_traced())
+        one.close()
+    paths = [rd.width * rd.height * rd.spp for _, rd in jobs]
+    big = [k for k, n in enumerate(paths) if n >= 1 << 22]
+    full_rate = sum(frame_rays[k] for k in big) / sum(frame_ms[k] for k in big)  # rays per ms
+    ideal_ms = sum(frame_rays) / full_rate
+    small = [k for k, n in enumerate(paths) if n < 1 << 20]
+    breakdown = {"frames_full_rate": len(big), "full_rate_mrays_s": round(full_rate / 1e3, 1),
+                 "plain_ideal_ms": round(ideal_ms, 2), "batching_bound": round(plain_ms / ideal_ms, 3),
+                 "batched_vs_ideal": round(ideal_ms / batch_ms, 3),
+                 "small_frames": len(small), "small_frames_rays_share": round(sum(frame_rays[k] for k in small) / sum(frame_rays), 4),
+                 "small_frames_time_share": round(sum(frame_ms[k] for k in small) / sum(frame_ms), 4),
+                 "frame_rays_sum_equals_batch": sum(frame_rays) == rays}
     return {"workload": f"{n_scenes} scenes (displaced icosphere + boxes, 1k-500k tris log-uniform), 64^2-512^2, 4/16/64 spp, depth 6, NEE",
             "tris": int(sum(sum(len(m.faces) for m in w[0]) for w in work)),
             "paths": int(sum(rd.width * rd.height * rd.spp for _, rd in jobs)), "rays": int(rays),
             "plain_ms": round(plain_ms, 2), "plain_mrays_s": round(rays / plain_ms / 1e3, 1),
             "plain_fused_ms": round(fused_ms, 2), "plain_fused_mrays_s": round(rays / fused_ms / 1e3, 1),
+            "plain_wavefront_ms": round(wavefront_ms, 2), "plain_wavefront_mrays_s": round(rays / wavefront_ms / 1e3, 1),
+            "plain_best_pick_ms": round(best_pick_ms, 2), "plain_best_pick_mrays_s": round(rays / best_pick_ms / 1e3, 1),
+            "speedup_vs_best_pick_plain": round(best_pick_ms / batch_ms, 3),
             "batched_ms": round(batch_ms, 2), "batched_mrays_s": round(rays / batch_ms / 1e3, 1),
             "speedup": round(plain_ms / batch_ms, 3), "speedup_vs_fused_plain": round(fused_ms / batch_ms, 3),
             "tuning": best.as_dict(), "autotune_trials": len(trials),
+            "plain_underfill": breakdown,
             "timing": "CUDA events around 256 sequential pt_render calls (device films; default pipeline = persistent "
-                      "path kernel, and PT_RENDER_FUSED) and around one batch graph replay"}
+                      "path kernel, PT_RENDER_FUSED and PT_RENDER_WAVEFRONT) and around one batch graph replay; best pick: "
+                      "per frame the faster of the default and the wavefront pipeline; plain_underfill: an event after "
+                      "each plain call (default pipeline), frames of >= 4,194,304 paths set the full rate"}
 
 
 def bench_render(pb, torch, cpu=True, cpu_rows=16, threads=None):
