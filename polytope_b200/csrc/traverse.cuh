@@ -32,7 +32,14 @@ struct RayState {
     float ix, iy, iz;          // 1/d (bvh.cpp:477-481)
     int kz;                    // Wald axis permutation (mesh.cpp:196-211): kx = kz+1, ky = kx+1 (mod 3)
     float sx, sy, sz;          // shear constants (mesh.cpp:234-236)
+    uint32_t neg;              // bit k: 1/d on axis k is < 0 (the child order, bvh.cpp:514-519)
 };
+
+// Whether the reference pushes the low child first at a node split on `axis` (1/d negative there).
+// A shift and a mask instead of selecting the axis's 1/d and comparing it per node step: on a B200
+// 1.3 M-face ray queries 2260 vs 2182 Mrays/s, the fused 6.5 M-face frame 989 vs 957 Msamples/s,
+// the 256-scene batch 2324 vs 2251-2264 Mrays/s (two runs each, same box).
+PT_HD bool neg_on(const RayState& r, uint32_t axis) { return (r.neg >> axis) & 1u; }
 
 PT_HD float sel3(int k, float x, float y, float z) { return k == 0 ? x : (k == 1 ? y : z); }
 PT_HD int next_axis(int k) { return k == 2 ? 0 : k + 1; }
@@ -42,6 +49,7 @@ PT_HD int next_axis(int k) { return k == 2 ? 0 : k + 1; }
 PT_HD void ray_setup(RayState& r, float ox, float oy, float oz, float dx, float dy, float dz) {
     r.ox = ox; r.oy = oy; r.oz = oz;
     r.ix = frcp(dx); r.iy = frcp(dy); r.iz = frcp(dz);
+    r.neg = (r.ix < 0 ? 1u : 0u) | (r.iy < 0 ? 2u : 0u) | (r.iz < 0 ? 4u : 0u);
     const float ax = fabs_(dx), ay = fabs_(dy), az = fabs_(dz);
     int kz = 0;
     if (ay > ax && ay > az) kz = 1;
@@ -320,7 +328,7 @@ PT_HD int walk_step(RayWalkT<CAP, SH>& k, const uint4* __restrict__ nodes, uint3
     }
     if (k.sp + 2 > CAP) return -1;
     const uint32_t axis = b.w >> 16;
-    const bool neg = (axis == 0 ? k.r.ix : (axis == 1 ? k.r.iy : k.r.iz)) < 0;
+    const bool neg = neg_on(k.r, axis);
     const uint32_t hi = ni + b.z, lo = ni + 1;
     k.stack.put(k.sp++, neg ? lo : hi);
     k.stack.put(k.sp++, neg ? hi : lo);
@@ -334,7 +342,6 @@ template <bool COUNT, int CAP, int SH>
 PT_HD bool walk_to_leaf(RayWalkT<CAP, SH>& k, const uint4* __restrict__ nodes, uint32_t num_nodes, uint32_t& leaf_off,
                         uint32_t& leaf_n) {
     leaf_n = 0;
-    const bool neg_x = k.r.ix < 0, neg_y = k.r.iy < 0, neg_z = k.r.iz < 0;
     while (k.sp > 0) {
         const uint32_t ni = k.stack.get(--k.sp);
         if (ni >= num_nodes) return false;
@@ -351,7 +358,7 @@ PT_HD bool walk_to_leaf(RayWalkT<CAP, SH>& k, const uint4* __restrict__ nodes, u
         }
         if (k.sp + 2 > CAP) return false;
         const uint32_t axis = b.w >> 16;
-        const bool neg = axis == 0 ? neg_x : (axis == 1 ? neg_y : neg_z);
+        const bool neg = neg_on(k.r, axis);
         const uint32_t hi = ni + b.z, lo = ni + 1;
         k.stack.put(k.sp++, neg ? lo : hi);
         k.stack.put(k.sp++, neg ? hi : lo);
@@ -435,7 +442,6 @@ PT_HD TraceResult traverse(const uint4* __restrict__ nodes, const float4* __rest
     res.u = res.v = res.w = 0.f;
     res.nodes = res.tris = 0;
     res.overflow = false;
-    const bool neg_x = r.ix < 0, neg_y = r.iy < 0, neg_z = r.iz < 0;
     const int box_mode = box_mode_for(r, tmax, exact_tree);
     uint32_t stack[CAP];
     int sp = 0;
@@ -468,7 +474,7 @@ PT_HD TraceResult traverse(const uint4* __restrict__ nodes, const float4* __rest
         }
         if (sp + 2 > CAP) { res.overflow = true; break; }
         const uint32_t axis = b.w >> 16;
-        const bool neg = axis == 0 ? neg_x : (axis == 1 ? neg_y : neg_z);
+        const bool neg = neg_on(r, axis);
         const uint32_t hi = ni + b.z, lo = ni + 1;
         stack[sp++] = neg ? lo : hi;
         stack[sp++] = neg ? hi : lo;

@@ -69,7 +69,6 @@ PT_HD TwoLevelHit traverse_two_level(const TwoLevelView& v, float ox, float oy, 
     out.inst = 0;
     RayState wr;
     ray_setup(wr, ox, oy, oz, dx, dy, dz);
-    const bool wneg_x = wr.ix < 0, wneg_y = wr.iy < 0, wneg_z = wr.iz < 0;
     const int wmode = box_mode_for(wr, tmax, v.exact_tree);
     float min_t = tmax;
     uint32_t tstack[kTopStackCap];
@@ -88,7 +87,7 @@ PT_HD TwoLevelHit traverse_two_level(const TwoLevelView& v, float ox, float oy, 
             if (tsp + 2 > kTopStackCap) { res.overflow = true; return out; }
             const uint32_t axis = b.w >> 16;
             const uint32_t hi = ti + b.z, lo = ti + 1;
-            const bool neg = axis == 0 ? wneg_x : (axis == 1 ? wneg_y : wneg_z);
+            const bool neg = neg_on(wr, axis);
             tstack[tsp++] = neg ? lo : hi;
             tstack[tsp++] = neg ? hi : lo;
             continue;
@@ -105,7 +104,6 @@ PT_HD TwoLevelHit traverse_two_level(const TwoLevelView& v, float ox, float oy, 
             to_object(w2o, dx, dy, dz, 0.0f, ldx, ldy, ldz);
             RayState r;
             ray_setup(r, lox, loy, loz, ldx, ldy, ldz);
-            const bool neg_x = r.ix < 0, neg_y = r.iy < 0, neg_z = r.iz < 0;
             const int mode = box_mode_for(r, min_t, v.exact_tree);
             int sp = 0;
             stack[sp++] = root;
@@ -138,7 +136,7 @@ PT_HD TwoLevelHit traverse_two_level(const TwoLevelView& v, float ox, float oy, 
                 }
                 if (sp + 2 > CAP) { res.overflow = true; return out; }
                 const uint32_t axis = nb.w >> 16;
-                const bool neg = axis == 0 ? neg_x : (axis == 1 ? neg_y : neg_z);
+                const bool neg = neg_on(r, axis);
                 const uint32_t hi = ni + nb.z, lo = ni + 1;
                 stack[sp++] = neg ? lo : hi;
                 stack[sp++] = neg ? hi : lo;
@@ -207,7 +205,7 @@ PT_HD int two_level_transition(RayWalkT<CAP, SH>& k, uint32_t e, const RenderPar
         }
         if (k.sp + 2 > CAP) return -1;
         const uint32_t axis = b.w >> 16;
-        const bool neg = (axis == 0 ? k.r.ix : (axis == 1 ? k.r.iy : k.r.iz)) < 0;
+        const bool neg = neg_on(k.r, axis);
         const uint32_t hi = ti + b.z, lo = ti + 1;
         k.stack.put(k.sp++, kTopTag | (neg ? lo : hi));
         k.stack.put(k.sp++, kTopTag | (neg ? hi : lo));
@@ -252,7 +250,7 @@ PT_HD int two_level_node_step(RayWalkT<CAP, SH>& k, uint32_t ni, const uint4* __
     }
     if (k.sp + 2 > CAP) return -1;
     const uint32_t axis = b.w >> 16;
-    const bool neg = (axis == 0 ? k.r.ix : (axis == 1 ? k.r.iy : k.r.iz)) < 0;
+    const bool neg = neg_on(k.r, axis);
     const uint32_t hi = ni + b.z, lo = ni + 1;
     k.stack.put(k.sp++, neg ? lo : hi);
     k.stack.put(k.sp++, neg ? hi : lo);
