@@ -4,6 +4,8 @@
 // HBM once (32 B in, 16 B out per ray); nodes and faces are read with 128-bit read-only loads and
 // stay resident in the 126 MB L2 for scenes up to a few million faces.
 
+#include <type_traits>
+
 #include "launch.h"
 #include "traverse.cuh"
 #include "two_level.cuh"
@@ -107,17 +109,27 @@ __global__ void __launch_bounds__(128, 8) trace_persistent_kernel(const uint4* _
             at_leaf = false;
             const uint32_t cand = __ballot_sync(0xFFFFFFFFu, active && k.sp > 0);
             const int want = __popc(cand) < PT_LEAF_BATCH_TRACE ? __popc(cand) : PT_LEAF_BATCH_TRACE;
-            while (true) {
-                const bool walking = active && ok && !at_leaf && k.sp > 0;
-                const uint32_t w = __ballot_sync(0xFFFFFFFFu, walking);
-                if (w == 0 || __popc(cand & ~w) >= want) break;
-                if (walking) {
-                    int r = walk_step<COUNT>(k, nodes, num_nodes, leaf_off, leaf_n);
-                    if (r == 0 && k.sp > 0) r = walk_step<COUNT>(k, nodes, num_nodes, leaf_off, leaf_n);
-                    at_leaf = r > 0;
-                    ok = r >= 0;
+            // the round's node steps, with the box test chosen once for the warp when every ray in
+            // it takes the min/max form (box_mode 0) instead of per step: 2437 vs 2337 Mrays/s on a
+            // B200 (1.3 M faces, 16.7 M rays)
+            auto round = [&](auto fast) {
+                constexpr bool kFast = decltype(fast)::value;
+                while (true) {
+                    const bool walking = active && ok && !at_leaf && k.sp > 0;
+                    const uint32_t w = __ballot_sync(0xFFFFFFFFu, walking);
+                    if (w == 0 || __popc(cand & ~w) >= want) break;
+                    if (walking) {
+                        int r = walk_step<COUNT, kFast>(k, nodes, num_nodes, leaf_off, leaf_n);
+                        if (r == 0 && k.sp > 0) r = walk_step<COUNT, kFast>(k, nodes, num_nodes, leaf_off, leaf_n);
+                        at_leaf = r > 0;
+                        ok = r >= 0;
+                    }
                 }
-            }
+            };
+            if (__all_sync(0xFFFFFFFFu, !active || k.box_mode == 0))
+                round(std::true_type{});
+            else
+                round(std::false_type{});
         } else {
             ok = !active || walk_to_leaf<COUNT>(k, nodes, num_nodes, leaf_off, leaf_n);
             at_leaf = active && ok && leaf_n > 0;

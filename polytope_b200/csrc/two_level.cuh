@@ -55,6 +55,54 @@ PT_HD void apply_point_dev(const float* m, float& x, float& y, float& z) {
     }
 }
 
+// One instance's bottom-level walk of traverse_two_level (the object-space ray `r`), with the box
+// test fixed for the ray (FAST: box_hits_fast) as in traverse_walk: the two-level 6.5 M-face frame
+// went from 836 to 1070 Msamples/s on a B200.  Returns 0 when the walk ends, 1 when an any-hit ray
+// accepted a face, -1 on a guard failure (res.overflow set).
+template <bool COUNT, int CAP, bool FAST>
+PT_HD int blas_walk(const TwoLevelView& v, const RayState& r, int mode, uint32_t root, uint32_t fbase, uint32_t pbase,
+                    uint32_t ii, bool any, uint32_t* stack, float& min_t, TwoLevelHit& out) {
+    TraceResult& res = out.r;
+    int sp = 0;
+    stack[sp++] = root;
+    while (sp > 0) {
+        const uint32_t ni = stack[--sp];
+        if (ni >= v.num_nodes) { res.overflow = true; return -1; }
+        uint4 na, nb;
+        ldg_node(v.nodes + 2 * (size_t)ni, na, nb);
+        if (COUNT) res.nodes++;
+        const bool hit = FAST ? box_hits_fast(r, bitsf(na.x), bitsf(na.y), bitsf(na.z), bitsf(na.w), bitsf(nb.x), bitsf(nb.y), min_t)
+                              : box_test(r, mode, bitsf(na.x), bitsf(na.y), bitsf(na.z), bitsf(na.w), bitsf(nb.x), bitsf(nb.y), min_t);
+        if (!hit) continue;
+        const uint32_t nfaces = nb.w & 0xFFFFu;
+        if (nfaces > 0) {
+            for (uint32_t j = 0; j < nfaces; ++j) {
+                const uint32_t face = fbase + nb.z + j;
+                const size_t fi = 3 * (size_t)face;
+                const float4 q0 = ldg_face(v.tris + fi), q1 = ldg_face(v.tris + fi + 1), q2 = ldg_face(v.tris + fi + 2);
+                if (COUNT) res.tris++;
+                float t, u, vv, w;
+                if (wald(r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, min_t, t, u, vv, w)) {
+                    min_t = t;
+                    res.prim = pbase + fbits(q2.y);
+                    res.leaf = face;
+                    res.t = t; res.u = u; res.v = vv; res.w = w;
+                    out.inst = ii;
+                    if (any) return 1;
+                }
+            }
+            continue;
+        }
+        if (sp + 2 > CAP) { res.overflow = true; return -1; }
+        const uint32_t axis = nb.w >> 16;
+        const bool neg = neg_on(r, axis);
+        const uint32_t hi = ni + nb.z, lo = ni + 1;
+        stack[sp++] = neg ? lo : hi;
+        stack[sp++] = neg ? hi : lo;
+    }
+    return 0;
+}
+
 template <bool COUNT, int CAP = kStackCap>
 PT_HD TwoLevelHit traverse_two_level(const TwoLevelView& v, float ox, float oy, float oz, float dx, float dy, float dz,
                                      float tmax, bool any) {
@@ -105,42 +153,9 @@ PT_HD TwoLevelHit traverse_two_level(const TwoLevelView& v, float ox, float oy, 
             RayState r;
             ray_setup(r, lox, loy, loz, ldx, ldy, ldz);
             const int mode = box_mode_for(r, min_t, v.exact_tree);
-            int sp = 0;
-            stack[sp++] = root;
-            while (sp > 0) {
-                const uint32_t ni = stack[--sp];
-                if (ni >= v.num_nodes) { res.overflow = true; return out; }
-                uint4 na, nb;
-                ldg_node(v.nodes + 2 * (size_t)ni, na, nb);
-                if (COUNT) res.nodes++;
-                if (!box_test(r, mode, bitsf(na.x), bitsf(na.y), bitsf(na.z), bitsf(na.w), bitsf(nb.x), bitsf(nb.y), min_t))
-                    continue;
-                const uint32_t nfaces = nb.w & 0xFFFFu;
-                if (nfaces > 0) {
-                    for (uint32_t j = 0; j < nfaces; ++j) {
-                        const uint32_t face = fbase + nb.z + j;
-                        const size_t fi = 3 * (size_t)face;
-                        const float4 q0 = ldg_face(v.tris + fi), q1 = ldg_face(v.tris + fi + 1), q2 = ldg_face(v.tris + fi + 2);
-                        if (COUNT) res.tris++;
-                        float t, u, vv, w;
-                        if (wald(r, q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, min_t, t, u, vv, w)) {
-                            min_t = t;
-                            res.prim = pbase + fbits(q2.y);
-                            res.leaf = face;
-                            res.t = t; res.u = u; res.v = vv; res.w = w;
-                            out.inst = ii;
-                            if (any) return out;
-                        }
-                    }
-                    continue;
-                }
-                if (sp + 2 > CAP) { res.overflow = true; return out; }
-                const uint32_t axis = nb.w >> 16;
-                const bool neg = neg_on(r, axis);
-                const uint32_t hi = ni + nb.z, lo = ni + 1;
-                stack[sp++] = neg ? lo : hi;
-                stack[sp++] = neg ? hi : lo;
-            }
+            const int st = mode == 0 ? blas_walk<COUNT, CAP, true>(v, r, 0, root, fbase, pbase, ii, any, stack, min_t, out)
+                                     : blas_walk<COUNT, CAP, false>(v, r, mode, root, fbase, pbase, ii, any, stack, min_t, out);
+            if (st != 0) return out;
         }
     }
     return out;
@@ -248,12 +263,11 @@ PT_HD int two_level_node_step(RayWalkT<CAP, SH>& k, uint32_t ni, const uint4* __
         leaf_n = nf;
         return 1;
     }
-    if (k.sp + 2 > CAP) return -1;
     const uint32_t axis = b.w >> 16;
     const bool neg = neg_on(k.r, axis);
     const uint32_t hi = ni + b.z, lo = ni + 1;
-    k.stack.put(k.sp++, neg ? lo : hi);
-    k.stack.put(k.sp++, neg ? hi : lo);
+    if (!k.stack.put2(k.sp, neg ? lo : hi, neg ? hi : lo)) return -1;
+    k.sp += 2;
     return 0;
 }
 

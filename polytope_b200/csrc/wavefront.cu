@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(128, PT_PATH_MIN_BLOCKS) wf_path_kernel(const 
                     }
                 }
             } else if constexpr (PT_LEAF_BATCH_PATHS > 0) {
-                walk_round<false, 1>(k, active && !finished && k.sp > 0, PT_LEAF_BATCH_PATHS, nodes, num_nodes, at_leaf,
+                walk_round<false, 1, true>(k, active && !finished && k.sp > 0, PT_LEAF_BATCH_PATHS, nodes, num_nodes, at_leaf,
                                      ok, leaf_off, leaf_n);
             } else {
                 const bool walking = active && !finished;
