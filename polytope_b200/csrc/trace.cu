@@ -49,6 +49,12 @@ __global__ void __launch_bounds__(128) trace_kernel(const uint4* __restrict__ no
 // the reference's; only which rays share a warp, and when a lane waits, changes.
 // 8 blocks of 128 per SM (64 registers, almost no spills) measured 2.6 % faster than 9 blocks at
 // 56 registers, where the warp vote's live state spilled.
+// Node steps a walking lane takes between ballots (a lane that reaches a leaf stops early).
+// Measured on a B200 (16.7 M microbench rays, two runs each, same box): 1 step 2142 -> 2 steps
+// (before the node-step changes); with them 2 steps 2428, 3 steps 2470, 4 steps 2067 Mrays/s.
+#ifndef PT_TRACE_STEPS
+#define PT_TRACE_STEPS 3
+#endif
 template <bool COUNT, int SH>
 __global__ void __launch_bounds__(128, 8) trace_persistent_kernel(const uint4* __restrict__ nodes,
                                                                const float4* __restrict__ tris, uint32_t num_nodes,
@@ -103,8 +109,8 @@ __global__ void __launch_bounds__(128, 8) trace_persistent_kernel(const uint4* _
         if constexpr (PT_LEAF_BATCH_TRACE > 0) {
             // walk_round (traverse.cuh), written out here: the compiler allocates this form with
             // fewer spills, which measured 9 % faster on the 1.3 M-face microbench; each lane takes
-            // up to two node steps per ballot (4.5 % faster than one: half the votes, and a lane
-            // that reaches a leaf on the first step skips the second)
+            // up to PT_TRACE_STEPS node steps per ballot (fewer votes; a lane that reaches a leaf
+            // skips the rest)
             ok = true;
             at_leaf = false;
             const uint32_t cand = __ballot_sync(0xFFFFFFFFu, active && k.sp > 0);
@@ -120,7 +126,9 @@ __global__ void __launch_bounds__(128, 8) trace_persistent_kernel(const uint4* _
                     if (w == 0 || __popc(cand & ~w) >= want) break;
                     if (walking) {
                         int r = walk_step<COUNT, kFast>(k, nodes, num_nodes, leaf_off, leaf_n);
-                        if (r == 0 && k.sp > 0) r = walk_step<COUNT, kFast>(k, nodes, num_nodes, leaf_off, leaf_n);
+#pragma unroll
+                        for (int extra = 1; extra < PT_TRACE_STEPS; ++extra)
+                            if (r == 0 && k.sp > 0) r = walk_step<COUNT, kFast>(k, nodes, num_nodes, leaf_off, leaf_n);
                         at_leaf = r > 0;
                         ok = r >= 0;
                     }
