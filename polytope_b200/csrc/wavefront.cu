@@ -151,8 +151,10 @@ __global__ void __launch_bounds__(256, kWfTraceMinBlocks) wf_trace_kernel(const 
         uint32_t leaf_off = 0, leaf_n = 0;
         bool ok, at_leaf;
         if constexpr (PT_LEAF_BATCH_WAVEFRONT > 0) {
-            // two node steps per ballot: 2152 vs 2028 Mrays/s on the 256-scene batch
-            walk_round<false, 2>(k, active && k.sp > 0, PT_LEAF_BATCH_WAVEFRONT, nodes, num_nodes, at_leaf, ok, leaf_off,
+            // node steps per ballot on the 256-scene batch: two 2152 vs one 2028 Mrays/s; after the
+            // node-step changes three 2438 vs two 2406 (the path kernel keeps one: two measured
+            // 1615 vs 1805 Msamples/s on the 6.5 M-face frame)
+            walk_round<false, 3>(k, active && k.sp > 0, PT_LEAF_BATCH_WAVEFRONT, nodes, num_nodes, at_leaf, ok, leaf_off,
                                  leaf_n);
         } else {
             ok = !active || walk_to_leaf<false, CAP>(k, nodes, num_nodes, leaf_off, leaf_n);
