@@ -252,8 +252,8 @@ constexpr int kShadeBatch = PT_SHADE_BATCH_PATHS;
 // Per-lane path state that only the shading step reads or writes (the path's next ray, throughput,
 // radiance, bounce count, the pending shadow contribution, the slot and its pixel, sample and
 // item), parked in shared memory between shading steps: the walk loop then holds only the ray
-// walk and the scene pointers in registers, so it runs at 8 blocks per SM without spilling its
-// state to local memory.  Field f of lane t lives at [f * 128 + t] (consecutive lanes, consecutive
+// walk and the scene pointers in registers, so it runs at 7 or 8 blocks per SM without spilling
+// that state to local memory.  Field f of lane t lives at [f * 128 + t] (consecutive lanes, consecutive
 // banks).
 enum ColdField : uint32_t {
     kOx, kOy, kOz, kDx, kDy, kDz, kSr, kSg, kSb, kLr, kLg, kLb, kCr, kCg, kCb,
@@ -292,9 +292,10 @@ struct TwoLevelLane {
     }
 };
 
-// 8 blocks of 128 per SM with the shading state in shared memory (see ColdField): on the 6.5 M-face
-// 1920x1080x64 frame 1840-1847 Msamples/s against 1794-1796 with that state in registers (and
-// spilled), and 1678 against 1584 Mrays/s on the 256-scene batch.  TL: the wave may hold
+// PT_PATH_MIN_BLOCKS blocks of 128 per SM.  With the shading state in shared memory (see
+// ColdField), at 8 blocks: on the 6.5 M-face 1920x1080x64 frame 1840-1847 Msamples/s against
+// 1794-1796 with that state in registers (and spilled), and 1678 against 1584 Mrays/s on the
+// 256-scene batch.  TL: the wave may hold
 // two-level scenes (a lane walks its item's layout: walk_step, or two_level_node_step and
 // two_level_transition).
 template <int CAP, int SH, bool TL>
