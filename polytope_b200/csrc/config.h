@@ -32,8 +32,8 @@
 // register allocator (blocks of 128 threads per SM).  With the lighter node steps (the box form
 // chosen per warp round, sign-mask child order, paired pushes) 7 blocks (72 registers) overtook 8
 // on a B200: the 6.5 M-face frame 1884-1888 against 1800-1805 Msamples/s, the saturated serving mix
-// 4624 against 4411 Mrays/s (the 256-scene plain frames 1551 against 1567); shade batches of 12 or
-// 24 measured 1706 / 1703.
+// 4624 against 4411 Mrays/s (the 256-scene plain frames 1551 against 1567); 6 blocks (80
+// registers) 1847 and 4574; shade batches of 12 or 24 measured 1706 / 1703 (at 8 blocks).
 #ifndef PT_SHADE_BATCH_PATHS
 #define PT_SHADE_BATCH_PATHS 16
 #endif
