@@ -248,15 +248,16 @@ PT_HD int two_level_transition(RayWalkT<CAP, SH>& k, uint32_t e, const RenderPar
 // A bottom-level node step: walk_step's test on an untagged entry the caller popped; at a hit
 // leaf the faces are leaf_off .. leaf_off + leaf_n - 1 counted from the current instance's first
 // face (face_base).  Returns 1 at a hit leaf, 0 otherwise, -1 on a guard failure.
-template <bool COUNT, int CAP, int SH>
+template <bool COUNT, bool FAST = false, int CAP, int SH>
 PT_HD int two_level_node_step(RayWalkT<CAP, SH>& k, uint32_t ni, const uint4* __restrict__ nodes, uint32_t num_nodes,
                               uint32_t& leaf_off, uint32_t& leaf_n) {
     if (ni >= num_nodes) return -1;
     uint4 a, b;
     ldg_node(nodes + 2 * (size_t)ni, a, b);
     if (COUNT) k.nodes++;
-    if (!box_test(k.r, k.box_mode, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), k.min_t))
-        return 0;
+    const bool hit = FAST ? box_hits_fast(k.r, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), k.min_t)
+                          : box_test(k.r, k.box_mode, bitsf(a.x), bitsf(a.y), bitsf(a.z), bitsf(a.w), bitsf(b.x), bitsf(b.y), k.min_t);
+    if (!hit) return 0;
     const uint32_t nf = b.w & 0xFFFFu;
     if (nf > 0) {
         leaf_off = b.z;
